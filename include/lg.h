@@ -1,0 +1,245 @@
+/*
+ * lg.h - C ABI of the B200 analytics engine for LLAMA multiversioned CSR stores.
+ *
+ * The reference (goatdb/llama) exposes its analytics path as header-only C++
+ * templates: the read-only multiversion graph `ll_mlcsr_ro_graph`
+ * (llama/include/llama/ll_mlcsr_graph.h:83), its iterator vocabulary
+ * (llama/include/llama/ll_mlcsr_iterator.h:53-214) and the benchmark task
+ * interface `ll_benchmark<Graph>::initialize/run/finalize`
+ * (benchmark/benchmarks/benchmark.h:127-319).  This header is the flat,
+ * pointer-and-size boundary that replaces those calls on one GPU: the host
+ * hands over levels in the reference's own in-memory format (vertex-table
+ * elements and 64-bit edge-table slots), and each analytics call runs as
+ * hand-written sm_100a kernels over a device-resident mirror of the level
+ * stack.
+ *
+ * Conventions
+ *   - Every function returns an lg_status (0 = LG_OK).  On error a message is
+ *     kept per thread; read it with lg_last_error().
+ *   - Output buffers may be host memory (pageable or pinned) or device memory
+ *     of the store's GPU.  With host outputs the call returns after the result
+ *     is copied back; with device outputs the work is only enqueued on the
+ *     store's stream and lg_store_sync() reports completion and deferred
+ *     errors.
+ *   - Calls on one store are serialised by the caller (one host thread at a
+ *     time, as the reference runs one benchmark at a time); distinct stores
+ *     are independent.
+ *   - No function falls back to a CPU implementation.  Without a usable GPU
+ *     lg_store_create() fails with LG_ECUDA.
+ */
+#ifndef LG_H_
+#define LG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------
+ * Status codes.  The reference prints and abort()s (llama/include/llama/
+ * ll_utils.h:394-416); the boundary reports instead.
+ * ------------------------------------------------------------------------- */
+typedef int lg_status;
+#define LG_OK        0
+#define LG_EINVAL    1   /* bad argument or malformed level                */
+#define LG_ENOMEM    2   /* device or pinned host allocation failed        */
+#define LG_ECUDA     3   /* CUDA runtime error, or no GPU                  */
+#define LG_ETIMEOUT  4   /* an iterative kernel hit its iteration/clock cap */
+#define LG_ESTATE    5   /* call not valid in the object's current state   */
+#define LG_ENOTSUP   6   /* configuration not supported by this build      */
+
+/* ---------------------------------------------------------------------------
+ * Bit layouts shared with the reference (64-bit node ids, LL_DELETIONS on).
+ *   edge id   = level << 38 | index          llama/include/llama/ll_mlcsr_helpers.h:55-83
+ *   slot      = payload | max_visible_level << 38
+ *                                             llama/include/llama/ll_mlcsr_helpers.h:90-114
+ *   a slot is visible in snapshot L iff max_visible_level > L
+ *   a freshly written slot has max_visible_level = 2^26 - 1
+ * ------------------------------------------------------------------------- */
+#define LG_BITS_LEVEL        26
+#define LG_BITS_INDEX        38
+#define LG_NIL_EDGE          ((int64_t)-1)
+#define LG_FRESH_MAX_LEVEL   ((1u << LG_BITS_LEVEL) - 1u)
+#define LG_EDGE_CREATE(level, index) \
+	((int64_t)(((uint64_t)(level) << LG_BITS_INDEX) | (uint64_t)(index)))
+#define LG_EDGE_LEVEL(e)     ((uint32_t)((uint64_t)(e) >> LG_BITS_INDEX))
+#define LG_EDGE_INDEX(e)     ((uint64_t)(e) & ((1ull << LG_BITS_INDEX) - 1ull))
+#define LG_SLOT_PAYLOAD(s)   ((uint64_t)(s) & ((1ull << LG_BITS_INDEX) - 1ull))
+#define LG_SLOT_MAX_LEVEL(s) ((uint32_t)((uint64_t)(s) >> LG_BITS_INDEX))
+
+/* Device limits of this build (checked at ingest, LG_ENOTSUP beyond them). */
+#define LG_MAX_LEVELS        64          /* levels per store                  */
+#define LG_MAX_FRAGMENT_LEN  ((1u << 26) - 1u) /* slots in one level fragment */
+
+/* Unreached vertex in BFS / SSSP outputs: INT_MAX - 1, the value the reference
+ * initialises with (benchmark/benchmarks/sssp.h:108, 289-293). */
+#define LG_UNREACHED         2147483646
+
+/* Vertex-table element, identical to ll_mlcsr_core__begin_t with
+ * LL_PRECOMPUTED_DEGREE (llama/include/llama/ll_mlcsr_helpers.h:141-149):
+ * start of this level's adjacency fragment (LG_NIL_EDGE if none), number of
+ * slots of that fragment, live out-degree at this level. */
+typedef struct lg_vt_entry {
+	int64_t  adj_list_start;
+	uint32_t level_length;
+	uint32_t degree;
+} lg_vt_entry;
+
+/* One CSR (out- or in-edges) of one level, as the reference holds it:
+ *   vt        max_nodes + 1 elements (the last one is the sentinel written by
+ *             finish_level_vertices, llama/include/llama/ll_mlcsr_sp.h:786-808);
+ *             alternatively vt_pages, the copy-on-write page table of
+ *             ll_mem_array_swcow (512 elements per page,
+ *             llama/include/llama/ll_mem_array.h:1019-1032); exactly one of
+ *             vt / vt_pages is non-NULL.
+ *   slots     the level's edge table, n_slots 64-bit slots (fragments followed
+ *             by their 16-byte continuation records for levels > 0,
+ *             llama/include/llama/ll_mlcsr_sp.h:1474-1497).
+ *   weights   optional per-slot edge property (NULL if none), read by SSSP
+ *             like ll_mlcsr_edge_property::get
+ *             (llama/include/llama/ll_mlcsr_properties.h:985-1017). */
+typedef struct lg_csr_level {
+	uint64_t                  max_nodes;
+	const lg_vt_entry*        vt;
+	const lg_vt_entry* const* vt_pages;
+	uint64_t                  n_slots;
+	const uint64_t*           slots;
+	const uint32_t*           weights;
+} lg_csr_level;
+
+/* A deletion recorded in an OLDER level's slot when this level was created:
+ * the reference lowers max_visible_level in place
+ * (update_max_visible_level_lower_only, llama/include/llama/ll_mlcsr_sp.h:849-863,
+ * called from llama/include/llama/ll_writable_graph.h:936-945). */
+typedef struct lg_deletion {
+	int64_t  edge;               /* LG_EDGE_CREATE(older level, slot index) */
+	uint32_t max_visible_level;  /* the new (lowered) value                  */
+	uint32_t reserved;
+} lg_deletion;
+
+/* Everything one new level adds to the store (the three things a checkpoint
+ * changes: a vertex-table level, an edge-table segment, deletion marks in
+ * older segments; llama/include/llama/ll_mlcsr_graph.h:1501-1831). */
+typedef struct lg_level_desc {
+	lg_csr_level        out;
+	lg_csr_level        in;           /* in.vt == in.vt_pages == NULL: no in-CSR */
+	const lg_deletion*  out_deletions;
+	uint64_t            n_out_deletions;
+	const lg_deletion*  in_deletions;
+	uint64_t            n_in_deletions;
+} lg_level_desc;
+
+typedef struct lg_store_opts {
+	int   device;        /* CUDA device ordinal                                 */
+	void* stream;        /* cudaStream_t to run on, or NULL for a private stream */
+	int   reverse_edges; /* 1: levels carry an in-CSR (LL_REVERSE_EDGES)        */
+	int   reserved;
+} lg_store_opts;
+
+typedef struct lg_store    lg_store;
+typedef struct lg_snapshot lg_snapshot;
+
+/* ---------------------------------------------------------------------------
+ * Store: device mirror of the level stack.
+ * Replaces ll_database / ll_mlcsr_ro_graph ownership of the levels
+ * (llama/include/llama/ll_database.h:51-149, ll_mlcsr_graph.h:83).
+ * ------------------------------------------------------------------------- */
+lg_status lg_store_create(lg_store** store, const lg_store_opts* opts);
+lg_status lg_store_destroy(lg_store* store);
+
+/* Append the next level (level number = lg_store_num_levels() before the
+ * call).  Mirrors what ll_mlcsr_ro_graph::checkpoint produces
+ * (llama/include/llama/ll_mlcsr_graph.h:1501-1831).  Host buffers are copied
+ * with pinned staging; the caller may free them on return. */
+lg_status lg_store_ingest_level(lg_store* store, const lg_level_desc* level);
+int       lg_store_num_levels(const lg_store* store);
+lg_status lg_store_max_nodes(const lg_store* store, int level, uint64_t* max_nodes);
+lg_status lg_store_sync(lg_store* store);
+/* The stream every call of this store runs on (a cudaStream_t). */
+void*     lg_store_stream(const lg_store* store);
+/* Device bytes held by the store (levels, deletions, snapshots). */
+uint64_t  lg_store_device_bytes(const lg_store* store);
+
+/* ---------------------------------------------------------------------------
+ * Snapshots.  A read-only view whose latest level is `level`, with deletions
+ * filtered at max_level = level: the snapshot constructor
+ * ll_mlcsr_ro_graph(master, level) (llama/include/llama/ll_mlcsr_graph.h:318-394)
+ * together with iter_begin(iter, n, level, max_level)
+ * (llama/include/llama/ll_mlcsr_sp.h:1994-2053).  Opening resolves every
+ * vertex's continuation chain into a fragment list (iter_descend,
+ * ll_mlcsr_sp.h:2090-2134) and builds the snapshot's deletion bitset.
+ * level = -1 selects the latest level.
+ * ------------------------------------------------------------------------- */
+lg_status lg_snapshot_open(lg_store* store, int level, lg_snapshot** snap);
+lg_status lg_snapshot_close(lg_snapshot* snap);
+lg_status lg_snapshot_level(const lg_snapshot* snap, int* level);
+lg_status lg_snapshot_max_nodes(const lg_snapshot* snap, uint64_t* max_nodes);
+/* Number of live edges (sum of out-degrees) of the snapshot. */
+lg_status lg_snapshot_num_edges(const lg_snapshot* snap, uint64_t* num_edges);
+
+/* Live out-degree per vertex, uint32[max_nodes]:
+ * ll_mlcsr_ro_graph::out_degree (llama/include/llama/ll_mlcsr_graph.h:726-741). */
+lg_status lg_out_degrees(lg_snapshot* snap, uint32_t* degrees);
+/* Live in-degree per vertex (requires the in-CSR). */
+lg_status lg_in_degrees(lg_snapshot* snap, uint32_t* degrees);
+
+/* Materialise the snapshot's adjacency in iteration order: for each vertex,
+ * newest fragment first, then older levels, deleted slots skipped - exactly
+ * the sequence ll_foreach_out / ll_foreach_in yield
+ * (llama/include/llama/ll_mlcsr_iterator.h:186-214).
+ * dir = 0 out-edges, 1 in-edges.  offsets: uint64[max_nodes + 1];
+ * neighbors: uint32[num edges]; edge_ids: int64 edge ids (may be NULL). */
+lg_status lg_snapshot_adjacency(lg_snapshot* snap, int dir, uint64_t* offsets,
+		uint32_t* neighbors, int64_t* edge_ids);
+
+/* ---------------------------------------------------------------------------
+ * Analytics kernels (the benchmark tasks of benchmark/benchmark.cc:871-946).
+ * ------------------------------------------------------------------------- */
+
+/* PageRank, pull direction, FP64: task "pagerank_double",
+ * ll_b_pagerank_pull_ext<Graph,double>::run (benchmark/benchmarks/pagerank.h:98-182).
+ * pr0 = 1/N with N = max_nodes; each of `iterations` steps sets
+ * pr'[t] = (1-d)/N + d * sum_{w in in(t)} pr[w] / out_degree(w); dangling mass
+ * is dropped.  ranks: double[max_nodes].  Requires the in-CSR. */
+lg_status lg_pagerank_pull(lg_snapshot* snap, int iterations, double damping,
+		double* ranks);
+
+/* BFS levels from `root`: u_sssp_bfs / ll_b_sssp_unweighted_bfs
+ * (benchmark/benchmarks/sssp.h:219-300) over ll_bfs_template
+ * (llama/include/llama/ll_bfs_template.h:152-293).  levels: int32[max_nodes],
+ * LG_UNREACHED for unreached vertices.  Direction-optimising: switches to
+ * bottom-up steps over the in-CSR when the frontier is large (levels are
+ * unique, so the result equals the reference's top-down BFS).
+ * result (may be NULL): reached = number of reached vertices, the "bfs_count"
+ * result (benchmark/benchmarks/bfs.h:117-127); reach_edges = sum of the
+ * out-degrees of the reached vertices (the Graph500 edge count used for
+ * GTEPS); max_level; and how many steps ran top-down and bottom-up. */
+typedef struct lg_bfs_result {
+	uint64_t reached;
+	uint64_t reach_edges;
+	int32_t  max_level;
+	int32_t  top_down_steps;
+	int32_t  bottom_up_steps;
+	int32_t  reserved;
+} lg_bfs_result;
+
+lg_status lg_bfs(lg_snapshot* snap, int64_t root, int32_t* levels,
+		lg_bfs_result* result);
+
+/* ---------------------------------------------------------------------------
+ * Errors.
+ * ------------------------------------------------------------------------- */
+/* Copies the calling thread's last error message (NUL-terminated, truncated
+ * to len); returns the message length. */
+size_t    lg_last_error(char* buf, size_t len);
+const char* lg_status_string(lg_status status);
+/* Version of this library, "major.minor.patch". */
+const char* lg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LG_H_ */

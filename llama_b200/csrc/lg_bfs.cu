@@ -1,0 +1,190 @@
+// lg_bfs.cu - breadth-first search levels over a snapshot.
+//
+// Reference: ll_bfs_template (llama/include/llama/ll_bfs_template.h:152-293)
+// driven by u_sssp_bfs / ll_b_sssp_unweighted_bfs
+// (benchmark/benchmarks/sssp.h:219-300): level-synchronous, top-down only,
+// dist[root] = 0, unreached vertices keep INT_MAX - 1.  BFS levels are
+// unique, so any level-synchronous traversal yields the same array; this one
+// is direction-optimising (Beamer et al., SC'12): top-down steps expand the
+// frontier queue over the out-CSR with warp_expand, bottom-up steps let every
+// unvisited vertex look for a parent among its in-neighbours (in-CSR) in a
+// frontier bitmap that stays resident in L2.
+#include "lg_device.cuh"
+
+namespace lg {
+
+constexpr int32_t kUnreached = LG_UNREACHED;
+constexpr int kBfsThreads = 256;
+
+__global__ void bfs_init(int32_t* level, uint64_t V, uint32_t root,
+		uint32_t* queue, const uint32_t* outdeg, unsigned long long* ctr) {
+	uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (v < V) level[v] = (v == root) ? 0 : kUnreached;
+	if (v == 0) {
+		queue[0] = root;
+		ctr[0] = 0;
+		ctr[1] = outdeg[root];
+	}
+}
+
+// Warp-aggregated append of `item` for the lanes with `take` set; returns
+// the number of items the warp appended.
+__device__ __forceinline__ void warp_append(bool take, uint32_t item,
+		uint32_t* queue, unsigned long long* len) {
+	unsigned m = __ballot_sync(0xffffffffu, take);
+	if (!m) return;
+	const uint32_t lane = threadIdx.x & 31u;
+	const int leader = __ffs(m) - 1;
+	unsigned long long base = 0;
+	if ((int)lane == leader) base = atomicAdd(len, (unsigned long long)__popc(m));
+	base = __shfl_sync(0xffffffffu, base, leader);
+	if (take) queue[base + __popc(m & ((1u << lane) - 1u))] = item;
+}
+
+__device__ __forceinline__ void warp_add_u64(unsigned long long x,
+		unsigned long long* dst) {
+	for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+	if ((threadIdx.x & 31) == 0 && x) atomicAdd(dst, x);
+}
+
+// ctr[0] = next frontier size, ctr[1] = sum of out-degrees of the next frontier
+__global__ void __launch_bounds__(kBfsThreads)
+bfs_top_down(SnapCsr out, const uint32_t* queue, uint32_t qlen,
+		int32_t* level, uint32_t* next, unsigned long long* ctr, int32_t cur) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint64_t i = ((uint64_t)blockIdx.x * (kBfsThreads / 32) + (threadIdx.x >> 5)) * 32 + lane;
+	const bool valid = i < qlen;
+	uint32_t cnt = 0, f0 = 0;
+	if (valid) cnt = vertex_slots(out, __ldg(queue + i), &f0);
+	unsigned long long mf = 0;
+	warp_expand(out, cnt, f0,
+		[&](bool act, uint32_t, uint32_t nbr, uint32_t, uint32_t) {
+			bool won = false;
+			if (act && __ldcg(level + nbr) == kUnreached)
+				won = atomicCAS(level + nbr, kUnreached, cur + 1) == kUnreached;
+			warp_append(won, nbr, next, ctr);
+			if (won) mf += __ldg(out.deg + nbr);
+		});
+	warp_add_u64(mf, ctr + 1);
+}
+
+__global__ void bfs_set_bits(const uint32_t* queue, uint32_t qlen, uint32_t* bits) {
+	uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= qlen) return;
+	uint32_t u = queue[i];
+	atomicOr(bits + (u >> 5), 1u << (u & 31));
+}
+
+__global__ void __launch_bounds__(kBfsThreads)
+bfs_bottom_up(SnapCsr in, const uint32_t* outdeg, const uint32_t* bits,
+		int32_t* level, uint32_t* next, unsigned long long* ctr, int32_t cur) {
+	const uint64_t v64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	const uint32_t v = (uint32_t)v64;
+	bool found = false;
+	if (v64 < in.V && level[v] == kUnreached) {
+		const uint32_t f0 = __ldg(in.frag_off + v), f1 = __ldg(in.frag_off + v + 1);
+		for (uint32_t f = f0; f < f1 && !found; f++) {
+			const uint2 fr = in.frags[f];
+			const uint32_t lv = frag_level(fr), n = frag_len(fr);
+			const uint32_t* ids = in.lt->ids[lv] + fr.x;
+			for (uint32_t k = 0; k < n; k++) {
+				uint32_t u = __ldg(ids + k);
+				if ((__ldg(bits + (u >> 5)) >> (u & 31)) & 1u) {
+					if (!slot_deleted(in.lt, lv, fr.x + k)) { found = true; break; }
+				}
+			}
+		}
+		if (found) level[v] = cur + 1;
+	}
+	warp_append(found, v, next, ctr);
+	warp_add_u64(found ? __ldg(outdeg + v) : 0ull, ctr + 1);
+}
+
+} // namespace lg
+
+using namespace lg;
+
+extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
+		lg_bfs_result* result) {
+	clear_error();
+	if (!sn || !levels) return set_error(LG_EINVAL, "null argument");
+	if (root < 0 || (uint64_t)root >= sn->V)
+		return set_error(LG_EINVAL, "root %lld out of range", (long long)root);
+	lg_store* s = sn->store;
+	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+	cudaStream_t st = s->stream;
+	const uint64_t V = sn->V;
+	DevBuf* sc = s->scratch;
+	LG_TRY(sc[0].reserve(V * 4));
+	LG_TRY(sc[1].reserve(V * 4));
+	LG_TRY(sc[2].reserve(((V + 31) / 32) * 4));
+	LG_TRY(sc[3].reserve(4 * sizeof(unsigned long long)));
+	const bool dev_out = is_device_pointer(levels);
+	int32_t* lvl = levels;
+	if (!dev_out) {
+		LG_TRY(sc[4].reserve(V * 4));
+		lvl = sc[4].as<int32_t>();
+	}
+	uint32_t* q = sc[0].as<uint32_t>();
+	uint32_t* nq = sc[1].as<uint32_t>();
+	uint32_t* bits = sc[2].as<uint32_t>();
+	unsigned long long* ctr = sc[3].as<unsigned long long>();
+	const SnapCsr out = sn->view(0);
+	const SnapCsr in = sn->in.present ? sn->view(1) : out;
+	const uint32_t* outdeg = sn->out.deg.as<uint32_t>();
+
+	bfs_init<<<grid_for(V, 256), 256, 0, st>>>(lvl, V, (uint32_t)root, q, outdeg, ctr);
+	LG_CUDA(cudaGetLastError(), "bfs_init");
+	unsigned long long h[2];
+	LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+	LG_CUDA(cudaStreamSynchronize(st), "bfs");
+	uint64_t qlen = 1, mf = h[1];
+	uint64_t mu = sn->out.n_edges - mf;   // edges out of unvisited vertices
+	uint64_t reached = 1, reach_edges = mf;
+	int32_t cur = 0;
+	int td_steps = 0, bu_steps = 0;
+	bool top_down = true;
+	const double alpha = 14.0, beta = 24.0;
+	while (qlen > 0) {
+		if (top_down && sn->in.present && (double)mf > (double)mu / alpha)
+			top_down = false;
+		else if (!top_down && (double)qlen < (double)V / beta)
+			top_down = true;
+		LG_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st), "memset");
+		if (top_down) {
+			uint64_t warps = (qlen + 31) / 32;
+			bfs_top_down<<<grid_for(warps, kBfsThreads / 32), kBfsThreads, 0, st>>>(
+					out, q, (uint32_t)qlen, lvl, nq, ctr, cur);
+			td_steps++;
+		} else {
+			LG_CUDA(cudaMemsetAsync(bits, 0, ((V + 31) / 32) * 4, st), "memset");
+			bfs_set_bits<<<grid_for(qlen, 256), 256, 0, st>>>(q, (uint32_t)qlen, bits);
+			bfs_bottom_up<<<grid_for(V, kBfsThreads), kBfsThreads, 0, st>>>(
+					in, outdeg, bits, lvl, nq, ctr, cur);
+			bu_steps++;
+		}
+		LG_CUDA(cudaGetLastError(), "bfs step");
+		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+		LG_CUDA(cudaStreamSynchronize(st), "bfs step");
+		qlen = h[0];
+		mf = h[1];
+		mu -= std::min(mu, (uint64_t)mf);
+		reached += qlen;
+		reach_edges += mf;
+		std::swap(q, nq);
+		cur++;
+	}
+	if (!dev_out) {
+		LG_TRY(copy_out(levels, lvl, V * 4, st));
+		LG_CUDA(cudaStreamSynchronize(st), "bfs");
+	}
+	if (result) {
+		result->reached = reached;
+		result->reach_edges = reach_edges;
+		result->max_level = cur - 1;
+		result->top_down_steps = td_steps;
+		result->bottom_up_steps = bu_steps;
+		result->reserved = 0;
+	}
+	return LG_OK;
+}

@@ -1,0 +1,242 @@
+// lg_device.cuh - device mirror of a LLAMA level stack and the warp-level
+// traversal primitive every analytics kernel is built on.
+//
+// Layout in HBM (one per CSR direction):
+//   level l:  vt[l]      (max_nodes_l + 1) x 16 B vertex-table elements, the
+//                        flattened copy-on-write table of that level
+//             ids[l]     n_slots_l x u32 neighbour ids; slots that are not
+//                        part of a fragment (continuation records, unused
+//                        continuation space) hold 0xffffffff and are never read
+//             w[l]       optional n_slots_l x u32 edge property
+//   deletions            every slot whose max_visible_level was lowered, as
+//                        (index, level << 26 | max_visible_level)
+// A snapshot L adds, per direction:
+//   frag_off   (V + 1) x u32   prefix of per-vertex fragment counts
+//   frags      F x uint2       {slot index, len << 6 | level}: the vertex's
+//                              continuation chain resolved newest-first
+//   del[l]     bitset over level l's slots, bit = max_visible_level <= L
+//   deg        V x u32         live degree (the vertex-table degree field)
+#ifndef LG_DEVICE_CUH_
+#define LG_DEVICE_CUH_
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "lg_internal.h"
+
+namespace lg {
+
+constexpr uint32_t kNoId = 0xffffffffu;
+constexpr int kLevelBits = 6;                 // level field of a fragment
+constexpr uint32_t kLevelMask = (1u << kLevelBits) - 1u;
+constexpr uint32_t kHubSlots = 4096;          // vertices with more slots are
+                                              // reduced by whole CTAs
+constexpr uint32_t kHubChunk = 4096;          // slots per hub CTA
+
+// Per-snapshot, per-direction table of level base pointers.
+struct LevelTab {
+	const uint32_t* ids[LG_MAX_LEVELS];
+	const uint32_t* del[LG_MAX_LEVELS];
+	const uint32_t* w[LG_MAX_LEVELS];
+};
+
+// What a kernel needs to walk one direction of a snapshot.
+struct SnapCsr {
+	const uint32_t* frag_off;   // V + 1
+	const uint2* frags;         // F
+	const LevelTab* lt;         // device copy
+	const uint32_t* deg;        // V
+	uint64_t V;
+};
+
+__device__ __forceinline__ uint32_t frag_len(uint2 f) { return f.y >> kLevelBits; }
+__device__ __forceinline__ uint32_t frag_level(uint2 f) { return f.y & kLevelMask; }
+
+__device__ __forceinline__ bool slot_deleted(const LevelTab* lt, uint32_t lv,
+		uint32_t idx) {
+	const uint32_t* d = lt->del[lv];
+	return (__ldg(d + (idx >> 5)) >> (idx & 31)) & 1u;
+}
+
+// Slots (live or deleted) of vertex v's fragments in this snapshot.
+__device__ __forceinline__ uint32_t vertex_slots(const SnapCsr& g, uint32_t v,
+		uint32_t* f0out) {
+	uint32_t f0 = __ldg(g.frag_off + v), f1 = __ldg(g.frag_off + v + 1);
+	uint32_t c = 0;
+	for (uint32_t f = f0; f < f1; f++) c += frag_len(g.frags[f]);
+	*f0out = f0;
+	return c;
+}
+
+// Warp-cooperative expansion.  Every lane brings one vertex (`cnt` slots
+// starting at fragment `f0`, cnt = 0 for none); the warp walks the union of
+// those slots 32 at a time, lane k taking the k-th slot of the chunk, so the
+// neighbour-id loads of a chunk are contiguous within each fragment.  For
+// every chunk `body(active, owner_lane, nbr, level, index)` runs on all 32
+// lanes (active = the lane holds a live slot), so the body may use warp
+// collectives.  Owners are non-decreasing across the lanes of a chunk.
+template <class Body>
+__device__ __forceinline__ void warp_expand(const SnapCsr& g, uint32_t cnt,
+		uint32_t f0, Body&& body) {
+	const uint32_t lane = threadIdx.x & 31u;
+	uint32_t incl = cnt;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+		if (lane >= (uint32_t)o) incl += t;
+	}
+	const uint32_t excl = incl - cnt;
+	const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+	for (uint32_t base = 0; base < total; base += 32) {
+		const uint32_t k = base + lane;
+		// owner = last lane whose range starts at or before k
+		uint32_t o = 0;
+#pragma unroll
+		for (uint32_t step = 16; step > 0; step >>= 1) {
+			uint32_t cand = o + step;
+			uint32_t e = __shfl_sync(0xffffffffu, excl, cand & 31u);
+			if (cand < 32 && e <= k) o = cand;
+		}
+		const uint32_t oexcl = __shfl_sync(0xffffffffu, excl, o);
+		uint32_t f = __shfl_sync(0xffffffffu, f0, o);
+		bool act = k < total;
+		uint32_t nbr = kNoId, lv = 0, idx = 0;
+		if (act) {
+			uint32_t r = k - oexcl;
+			uint2 fr = g.frags[f];
+			while (r >= frag_len(fr)) { r -= frag_len(fr); fr = g.frags[++f]; }
+			lv = frag_level(fr);
+			idx = fr.x + r;
+			act = !slot_deleted(g.lt, lv, idx);
+			if (act) nbr = __ldg(g.lt->ids[lv] + idx);
+		}
+		body(act, o, nbr, lv, idx);
+	}
+}
+
+// Warp inclusive segmented sum of `v` over lanes with equal `key` (keys are
+// non-decreasing); returns the sum at each lane and sets *tail for the last
+// lane of every segment.
+__device__ __forceinline__ double warp_segsum(double v, uint32_t key, bool* tail) {
+	const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		double t = __shfl_up_sync(0xffffffffu, v, o);
+		uint32_t k = __shfl_up_sync(0xffffffffu, key, o);
+		if (lane >= (uint32_t)o && k == key) v += t;
+	}
+	uint32_t nk = __shfl_down_sync(0xffffffffu, key, 1);
+	*tail = (lane == 31u) || (nk != key);
+	return v;
+}
+
+// ---------------------------------------------------------------------------
+// Host-side objects
+// ---------------------------------------------------------------------------
+
+// Device allocation owned by a host object.
+struct DevBuf {
+	void* p = nullptr;
+	size_t bytes = 0;
+	DevBuf() = default;
+	DevBuf(const DevBuf&) = delete;
+	DevBuf& operator=(const DevBuf&) = delete;
+	~DevBuf() { release(); }
+	void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+	// (Re)allocate to at least n bytes; contents are not preserved.
+	lg_status reserve(size_t n);
+	template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct DevLevel {
+	uint64_t max_nodes = 0;
+	uint64_t n_slots = 0;
+	DevBuf vt;        // lg_vt_entry[max_nodes + 1]
+	DevBuf ids;       // u32[n_slots]
+	DevBuf w;         // u32[n_slots] or empty
+};
+
+struct DevCsr {
+	std::vector<DevLevel*> levels;
+	std::vector<uint2> dels_host;   // (index, level << 26 | max_visible_level)
+	DevBuf dels;                    // device copy of dels_host
+	uint64_t n_dels_dev = 0;
+	~DevCsr() { for (DevLevel* l : levels) delete l; }
+};
+
+struct SnapDir {
+	DevBuf frag_off, frags, deg, delbits, lt, hubs, hub_chunk_off;
+	uint64_t n_frags = 0;
+	uint64_t n_edges = 0;          // live edges (sum of degrees)
+	uint32_t n_hubs = 0;
+	uint32_t n_hub_chunks = 0;
+	bool present = false;
+	SnapCsr view() const {
+		SnapCsr s;
+		s.frag_off = frag_off.as<uint32_t>();
+		s.frags = frags.as<uint2>();
+		s.lt = lt.as<LevelTab>();
+		s.deg = deg.as<uint32_t>();
+		s.V = 0;
+		return s;
+	}
+};
+
+} // namespace lg
+
+struct lg_store {
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	bool own_stream = false;
+	bool reverse = false;
+	lg::DevCsr out, in;
+	// pinned staging for host -> device copies (two halves, double-buffered)
+	void* pinned = nullptr;
+	size_t pinned_bytes = 0;
+	cudaEvent_t staged[2] = {nullptr, nullptr};
+	// scratch shared by the analytics calls of this store
+	lg::DevBuf scratch[8];
+	int open_snapshots = 0;
+};
+
+struct lg_snapshot {
+	lg_store* store = nullptr;
+	int level = 0;
+	uint64_t V = 0;
+	lg::SnapDir out, in;
+	lg::SnapCsr view(int dir) const {
+		lg::SnapCsr s = (dir == 0 ? out : in).view();
+		s.V = V;
+		return s;
+	}
+};
+
+namespace lg {
+
+// CUDA error -> lg_status with a message naming the failing step.
+lg_status cuda_status(cudaError_t e, const char* what);
+#define LG_CUDA(call, what) do { cudaError_t _e = (call); \
+	if (_e != cudaSuccess) return ::lg::cuda_status(_e, what); } while (0)
+#define LG_TRY(expr) do { lg_status _s = (expr); if (_s) return _s; } while (0)
+
+// True if p is device (or managed) memory usable by the store's GPU.
+bool is_device_pointer(const void* p);
+
+// Exclusive scan of n u32 counts into out[0..n] (u32); returns false if the
+// total does not fit 32 bits.  Runs on `stream`, uses `tmp` as scratch.
+lg_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n,
+		DevBuf& tmp, cudaStream_t stream, uint64_t* total);
+
+// Copy `bytes` of device data to a caller buffer (host or device).
+lg_status copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
+inline unsigned grid_for(uint64_t n, unsigned block) {
+	uint64_t g = (n + block - 1) / block;
+	return (unsigned)(g > 0x7fffffffull ? 0x7fffffffull : (g == 0 ? 1 : g));
+}
+
+} // namespace lg
+
+#endif // LG_DEVICE_CUH_

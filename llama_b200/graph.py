@@ -1,0 +1,248 @@
+"""Python mirror of the LLAMA analytics interface over liblg.
+
+Names follow the reference: a ``HostGraph`` plays the writable side that
+checkpoints levels (``ll_writable_graph::checkpoint``), a ``Store`` the
+``ll_database`` that owns the read-only level stack, a ``Snapshot`` the view
+``ll_mlcsr_ro_graph(master, level)``, and the analytics methods are the
+benchmark tasks of ``benchmark -r <task>`` (benchmark/benchmark.cc:871-946).
+Every call goes through the C ABI in include/lg.h; results come back as numpy
+arrays, or are written into caller-provided torch CUDA tensors.
+"""
+import ctypes as C
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib, ptr
+
+
+@dataclass
+class GraphSpec:
+    """Seeded synthetic multiversion graph (``lg_graph_spec``)."""
+    scale: int
+    edge_factor: float = 16.0
+    a: float = 0.57
+    b: float = 0.19
+    c: float = 0.19
+    seed: int = 1
+    kind: int = _lib.LG_GEN_RMAT
+    symmetrize: bool = False
+    num_levels: int = 1
+    level0_fraction: float = 1.0
+    delete_fraction: float = 0.0
+    split_seed: int = 0
+    weight_max: int = 0
+    weight_seed: int = 0
+
+    def to_c(self):
+        s = _lib.lg_graph_spec()
+        for f in fields(self):
+            setattr(s, f.name, int(getattr(self, f.name))
+                    if isinstance(getattr(self, f.name), bool) else getattr(self, f.name))
+        return s
+
+    @property
+    def max_nodes(self):
+        return 1 << self.scale
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+class HostGraph:
+    """Host-side multiversion graph in the reference's level layout."""
+
+    def __init__(self, max_nodes, reverse_edges=True):
+        h = C.c_void_p()
+        check(lib.lg_hgraph_create(C.byref(h), int(max_nodes), int(bool(reverse_edges))))
+        self._h = h
+        self.max_nodes = int(max_nodes)
+        self.reverse_edges = bool(reverse_edges)
+
+    @classmethod
+    def from_spec(cls, spec, reverse_edges=True):
+        g = cls(spec.max_nodes, reverse_edges)
+        check(lib.lg_hgraph_build(g._h, C.byref(spec.to_c())))
+        return g
+
+    def close(self):
+        if self._h:
+            lib.lg_hgraph_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def num_levels(self):
+        return lib.lg_hgraph_num_levels(self._h)
+
+    def add_level(self, src, dst, del_src=(), del_dst=(), weights=None):
+        src, dst = _u32(src), _u32(dst)
+        ds, dd = _u32(del_src), _u32(del_dst)
+        w = None if weights is None else _u32(weights)
+        check(lib.lg_hgraph_add_level(self._h, ptr(src), ptr(dst), len(src),
+                                      ptr(ds), ptr(dd), len(ds), ptr(w)))
+
+    def level_input(self, level):
+        """(src, dst, del_src, del_dst, weights) the level was built from."""
+        ps, pd, pds, pdd, pw = (C.c_void_p() for _ in range(5))
+        n, nd = C.c_uint64(), C.c_uint64()
+        check(lib.lg_hgraph_level_input(self._h, level, C.byref(ps), C.byref(pd),
+                                        C.byref(n), C.byref(pds), C.byref(pdd),
+                                        C.byref(nd), C.byref(pw)))
+
+        def arr(p, k):
+            if k == 0 or not p.value:
+                return np.zeros(0, np.uint32)
+            return np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint32)), (k,)).copy()
+        w = arr(pw, n.value) if pw.value else None
+        return (arr(ps, n.value), arr(pd, n.value), arr(pds, nd.value),
+                arr(pdd, nd.value), w)
+
+    def level_desc(self, level):
+        d = _lib.lg_level_desc()
+        check(lib.lg_hgraph_level_desc(self._h, level, C.byref(d)))
+        return d
+
+    def level_arrays(self, level, direction=0):
+        """(vertex table, slots) of one level as numpy copies."""
+        d = self.level_desc(level)
+        c = d.out if direction == 0 else d.in_
+        vt = np.ctypeslib.as_array(C.cast(c.vt, C.POINTER(C.c_uint8)),
+                                   ((c.max_nodes + 1) * 16,)).copy().view(_lib.VT_DTYPE)
+        if c.n_slots:
+            sl = np.ctypeslib.as_array(C.cast(c.slots, C.POINTER(C.c_uint64)),
+                                       (c.n_slots,)).copy()
+        else:
+            sl = np.zeros(0, np.uint64)
+        return vt, sl
+
+
+class Store:
+    """Device mirror of the level stack (``lg_store``)."""
+
+    def __init__(self, device=0, stream=None, reverse_edges=True):
+        o = _lib.lg_store_opts(device=device, stream=stream or None,
+                               reverse_edges=int(bool(reverse_edges)))
+        h = C.c_void_p()
+        check(lib.lg_store_create(C.byref(h), C.byref(o)))
+        self._h = h
+        self.reverse_edges = bool(reverse_edges)
+
+    def close(self):
+        if self._h:
+            check(lib.lg_store_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def num_levels(self):
+        return lib.lg_store_num_levels(self._h)
+
+    @property
+    def stream(self):
+        return lib.lg_store_stream(self._h)
+
+    @property
+    def device_bytes(self):
+        return lib.lg_store_device_bytes(self._h)
+
+    def ingest(self, hgraph, first=None):
+        first = self.num_levels if first is None else first
+        check(lib.lg_hgraph_ingest(hgraph.handle, self._h, first))
+
+    def ingest_level(self, desc):
+        check(lib.lg_store_ingest_level(self._h, C.byref(desc)))
+
+    def sync(self):
+        check(lib.lg_store_sync(self._h))
+
+    def snapshot(self, level=-1):
+        return Snapshot(self, level)
+
+
+class Snapshot:
+    """Read-only view of one level (``lg_snapshot``)."""
+
+    def __init__(self, store, level=-1):
+        h = C.c_void_p()
+        check(lib.lg_snapshot_open(store.handle, level, C.byref(h)))
+        self._h = h
+        self.store = store
+        lv, mn = C.c_int(), C.c_uint64()
+        check(lib.lg_snapshot_level(h, C.byref(lv)))
+        check(lib.lg_snapshot_max_nodes(h, C.byref(mn)))
+        self.level = lv.value
+        self.max_nodes = mn.value
+
+    def close(self):
+        if self._h:
+            check(lib.lg_snapshot_close(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def num_edges(self):
+        n = C.c_uint64()
+        check(lib.lg_snapshot_num_edges(self._h, C.byref(n)))
+        return n.value
+
+    def out_degrees(self):
+        out = np.empty(self.max_nodes, np.uint32)
+        check(lib.lg_out_degrees(self._h, ptr(out)))
+        return out
+
+    def in_degrees(self):
+        out = np.empty(self.max_nodes, np.uint32)
+        check(lib.lg_in_degrees(self._h, ptr(out)))
+        return out
+
+    def adjacency(self, direction=0, with_edge_ids=False):
+        """(offsets, neighbours[, edge ids]) in the reference's iteration order."""
+        off = np.empty(self.max_nodes + 1, np.uint64)
+        check(lib.lg_snapshot_adjacency(self._h, direction, ptr(off), None, None))
+        n = int(off[-1])
+        nb = np.empty(max(n, 1), np.uint32)
+        ei = np.empty(max(n, 1), np.int64) if with_edge_ids else None
+        check(lib.lg_snapshot_adjacency(self._h, direction, ptr(off), ptr(nb), ptr(ei)))
+        if with_edge_ids:
+            return off, nb[:n], ei[:n]
+        return off, nb[:n]
+
+    # ---- benchmark tasks -------------------------------------------------
+    def pagerank_pull(self, iterations=10, damping=0.85, out=None):
+        """Task ``pagerank_double``: FP64 pull PageRank."""
+        res = np.empty(self.max_nodes, np.float64) if out is None else out
+        check(lib.lg_pagerank_pull(self._h, int(iterations), float(damping), ptr(res)))
+        return res
+
+    def bfs(self, root, out=None):
+        """Task ``sssp_unweighted`` (BFS levels); returns (levels, lg_bfs_result)."""
+        res = np.empty(self.max_nodes, np.int32) if out is None else out
+        r = _lib.lg_bfs_result()
+        check(lib.lg_bfs(self._h, int(root), ptr(res), C.byref(r)))
+        return res, r

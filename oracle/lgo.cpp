@@ -1,0 +1,374 @@
+// lgo.cpp - CPU ORACLE for the LLAMA analytics path.
+//
+// TEST INFRASTRUCTURE ONLY.  This file restates, serially and plainly, the
+// reference's multiversioned CSR and its benchmark kernels so that the CUDA
+// engine (llama_b200/) can be checked against it.  Only tests/, the smoke
+// check and the CPU-baseline leg of bench.py may load it; the product never
+// does.  It is itself pinned against the reference code compiled from source
+// (oracle/ref_harness.cc -> oracle/_ref/) and against the committed golden
+// fixtures in tests/golden/.
+//
+// Every function names the reference lines it restates (paths relative to
+// the goatdb/llama source tree).
+
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <queue>
+#include <vector>
+
+namespace {
+
+const int BITS_LEVEL = 26;                          // ll_mlcsr_helpers.h:62
+const int BITS_INDEX = 64 - BITS_LEVEL;             // ll_mlcsr_helpers.h:68
+const int64_t NIL = -1;                             // ll_common.h:118-120
+const uint64_t FRESH = (1ull << BITS_LEVEL) - 1;    // LL_MAX_LEVEL + 2, :102
+const int32_t UNREACHED = 2147483646;               // INT_MAX - 1, sssp.h:108
+
+inline int64_t edge_create(uint64_t level, uint64_t index) {   // :76
+	return (int64_t)((level << BITS_INDEX) | index);
+}
+inline uint64_t edge_level(int64_t e) { return (uint64_t)e >> BITS_INDEX; }       // :77
+inline uint64_t edge_index(int64_t e) { return (uint64_t)e & ((1ull << BITS_INDEX) - 1); } // :78
+inline uint64_t value_create_ext(uint64_t payload, uint64_t maxlev) {  // :98-101
+	return payload | (maxlev << BITS_INDEX);
+}
+inline uint64_t value_payload(uint64_t x) { return x & ((1ull << BITS_INDEX) - 1); } // :104
+inline uint64_t value_max_level(uint64_t x) { return x >> BITS_INDEX; }              // :105
+inline bool value_is_deleted(uint64_t x, uint64_t level) {                           // :107
+	return value_max_level(x) <= level;
+}
+
+struct VtEntry {            // ll_mlcsr_core__begin_t, ll_mlcsr_helpers.h:141-149
+	int64_t adj_list_start;
+	uint32_t level_length;
+	uint32_t degree;
+};
+
+struct Csr {
+	std::vector<std::vector<VtEntry>> vt;     // per level, max_nodes + 1
+	std::vector<std::vector<uint64_t>> et;    // per level edge table
+	std::vector<std::vector<uint32_t>> w;     // per level edge property
+};
+
+struct Iter {               // ll_edge_iterator, ll_mlcsr_iterator.h:53-68
+	int64_t edge;
+	uint64_t left;
+	uint64_t ptr_level, ptr_index;
+	int64_t node;
+	int64_t last_node;
+	uint64_t max_level;
+};
+
+// iter_descend, ll_mlcsr_sp.h:2090-2134: the continuation record is the
+// 16 bytes right after the last slot of the fragment.
+void iter_descend(const Csr& c, Iter& it) {
+	uint64_t level = edge_level(it.edge);
+	if (level == 0 || (uint64_t)it.node >= c.vt[level - 1].size() - 1) {
+		it.edge = NIL;
+		return;
+	}
+	VtEntry b;
+	memcpy(&b, &c.et[it.ptr_level][it.ptr_index + 1], sizeof(b));
+	it.edge = b.adj_list_start;
+	it.left = b.level_length;
+	if (it.left == 0) it.edge = NIL;
+	else { it.ptr_level = edge_level(it.edge); it.ptr_index = edge_index(it.edge); }
+}
+
+// is_edge_deleted, ll_mlcsr_sp.h:1290-1310
+bool is_deleted(const Csr& c, const Iter& it) {
+	if (it.edge == NIL) return false;
+	uint64_t v = c.et[edge_level(it.edge)][edge_index(it.edge)];
+	return value_is_deleted(v, it.max_level);
+}
+
+// iter_next, ll_mlcsr_sp.h:2145-2196
+int64_t iter_next(const Csr& c, Iter& it) {
+	int64_t r = it.edge;
+	if (r != NIL) {
+		it.last_node = (int64_t)value_payload(c.et[it.ptr_level][it.ptr_index]);
+		do {
+			if (it.left > 1) {
+				it.left--;
+				it.edge = it.edge + 1;
+				it.ptr_index++;
+			} else {
+				iter_descend(c, it);
+			}
+		} while (is_deleted(c, it));
+	}
+	return r;
+}
+
+// iter_begin, ll_mlcsr_sp.h:1994-2053 (level = snapshot, max_level = level)
+void iter_begin(const Csr& c, Iter& it, int64_t n, int level) {
+	it.node = n;
+	it.max_level = level;
+	const VtEntry& b = c.vt[level][n];
+	it.edge = b.adj_list_start;
+	it.left = b.level_length;
+	if (it.left == 0) it.edge = NIL;
+	else { it.ptr_level = edge_level(it.edge); it.ptr_index = edge_index(it.edge); }
+	if (is_deleted(c, it)) {
+		int64_t keep = it.last_node;
+		iter_next(c, it);
+		it.last_node = keep;
+	}
+}
+
+// Neighbours in iteration order (ll_foreach_out / ll_foreach_in,
+// ll_mlcsr_iterator.h:186-214), with the edge id of each.
+void neighbours(const Csr& c, int level, int64_t n, std::vector<uint32_t>& nb,
+		std::vector<int64_t>* ids) {
+	nb.clear();
+	if (ids) ids->clear();
+	Iter it;
+	it.last_node = -1;
+	iter_begin(c, it, n, level);
+	for (int64_t e = iter_next(c, it); e != NIL; e = iter_next(c, it)) {
+		nb.push_back((uint32_t)it.last_node);
+		if (ids) ids->push_back(e);
+	}
+}
+
+// find, ll_mlcsr_sp.h:2334-2356: first edge of n whose payload is `value`.
+int64_t find_edge(const Csr& c, int level, int64_t n, uint64_t value) {
+	Iter it;
+	it.last_node = -1;
+	iter_begin(c, it, n, level);
+	for (int64_t e = iter_next(c, it); e != NIL; e = iter_next(c, it))
+		if ((uint64_t)it.last_node == value) return e;
+	return NIL;
+}
+
+// One level of one CSR: init_level_from_degrees (ll_mlcsr_sp.h:1562-1607)
+// -> init_node per vertex (:1375-1550) -> finish_level_vertices (:786-808),
+// then write_value for every new edge (:1618-1627), fragments sorted by
+// target.  `adj[v]` are the new neighbours of v (sorted), `del[v]` the number
+// of v's edges this level deletes.
+void build_level(Csr& c, uint64_t V, const std::vector<std::vector<uint32_t>>& adj,
+		const std::vector<uint32_t>& del, const std::vector<std::vector<uint32_t>>* wts) {
+	const int level = (int)c.vt.size();
+	std::vector<VtEntry> vt;
+	uint64_t prev_size = 0;
+	if (level > 0) {
+		vt = c.vt[level - 1];                     // copy-on-write: start shared
+		prev_size = vt.size() - 1;
+		VtEntry zero = {0, 0, 0};
+		vt.resize(V + 1, zero);
+	} else {
+		VtEntry nil = {NIL, 0, 0};
+		vt.assign(V + 1, nil);
+	}
+	const std::vector<VtEntry>* prev = level > 0 ? &c.vt[level - 1] : nullptr;
+	std::vector<uint64_t> et;
+	std::vector<uint32_t> wt;
+	uint64_t write_index = 0;
+	std::vector<uint64_t> start(V, 0);
+	for (uint64_t node = 0; node < V; node++) {
+		uint64_t new_edges = adj[node].size();
+		uint64_t deleted = level == 0 ? 0 : del[node];
+		VtEntry e = {0, 0, 0};
+		if (!(level == 0 || new_edges > 0 || deleted > 0)) {
+			if (node >= prev_size) { e.adj_list_start = NIL; vt[node] = e; }
+			continue;
+		}
+		if (level == 0 || new_edges > 0) {
+			e.adj_list_start = new_edges == 0 ? NIL : edge_create(level, write_index);
+			e.level_length = (uint32_t)new_edges;
+		} else {
+			if (node >= prev_size) e.adj_list_start = NIL;
+			else e = (*prev)[node];
+		}
+		e.degree = (uint32_t)(new_edges - deleted);
+		if (level > 0 && node < prev_size) {
+			const VtEntry& bprev = (*prev)[node];
+			if (bprev.adj_list_start != NIL) e.degree = e.degree + bprev.degree;
+		}
+		if (e.degree == 0) { e.adj_list_start = NIL; e.level_length = 0; }
+		uint64_t delta = new_edges;
+		start[node] = write_index;
+		if (level > 0 && e.adj_list_start != NIL) {
+			uint64_t t = write_index + new_edges;
+			VtEntry x = {NIL, 0, 0};
+			if (node < prev_size) x = (*prev)[node];
+			if (et.size() < t + 2) { et.resize(t + 2, 0); wt.resize(t + 2, 0); }
+			memcpy(&et[t], &x, sizeof(x));
+			delta += 2;
+		}
+		vt[node] = e;
+		write_index += delta;
+	}
+	VtEntry sentinel = {edge_create(level, write_index), 0, 0};
+	vt[V] = sentinel;
+	et.resize(write_index, 0);
+	wt.resize(write_index, 0);
+	for (uint64_t node = 0; node < V; node++)
+		for (uint64_t k = 0; k < adj[node].size(); k++) {
+			et[start[node] + k] = value_create_ext(adj[node][k], FRESH);
+			if (wts) wt[start[node] + k] = (*wts)[node][k];
+		}
+	c.vt.push_back(std::move(vt));
+	c.et.push_back(std::move(et));
+	c.w.push_back(std::move(wt));
+}
+
+struct Graph {
+	uint64_t V;
+	Csr out, in;
+};
+
+} // namespace
+
+extern "C" {
+
+void* lgo_create(uint64_t V) {
+	Graph* g = new Graph();
+	g->V = V;
+	return g;
+}
+
+void lgo_destroy(void* g) { delete (Graph*)g; }
+
+int lgo_num_levels(void* gp) { return (int)((Graph*)gp)->out.vt.size(); }
+
+// Append a level: new edges (any order), deleted edges (live in the latest
+// snapshot), optional weights per new edge.  Deletions lower the slot's
+// max_visible_level to the new level number in both CSRs
+// (update_max_visible_level_lower_only, ll_mlcsr_sp.h:849-863, as called
+// from ll_writable_graph.h:936-945).  Returns 0 or -1 on bad input.
+int lgo_add_level(void* gp, const uint32_t* src, const uint32_t* dst, uint64_t n,
+		const uint32_t* dsrc, const uint32_t* ddst, uint64_t nd,
+		const uint32_t* weights) {
+	Graph* g = (Graph*)gp;
+	const uint64_t V = g->V;
+	const int level = (int)g->out.vt.size();
+	std::vector<std::vector<uint32_t>> oadj(V), iadj(V), ow(V);
+	std::vector<std::pair<std::pair<uint32_t, uint32_t>, uint32_t>> e(n);
+	for (uint64_t i = 0; i < n; i++) {
+		if (src[i] >= V || dst[i] >= V) return -1;
+		e[i] = {{src[i], dst[i]}, weights ? weights[i] : 0u};
+	}
+	std::sort(e.begin(), e.end());
+	for (uint64_t i = 0; i < n; i++) {
+		oadj[e[i].first.first].push_back(e[i].first.second);
+		ow[e[i].first.first].push_back(e[i].second);
+	}
+	for (uint64_t i = 0; i < n; i++) iadj[e[i].first.second].push_back(e[i].first.first);
+	std::vector<uint32_t> odel(V, 0), idel(V, 0);
+	std::vector<int64_t> oe(nd), ie(nd);
+	for (uint64_t i = 0; i < nd; i++) {
+		if (level == 0) return -1;
+		oe[i] = find_edge(g->out, level - 1, dsrc[i], ddst[i]);
+		ie[i] = find_edge(g->in, level - 1, ddst[i], dsrc[i]);
+		if (oe[i] == NIL || ie[i] == NIL) return -1;
+		odel[dsrc[i]]++;
+		idel[ddst[i]]++;
+	}
+	build_level(g->out, V, oadj, odel, weights ? &ow : nullptr);
+	build_level(g->in, V, iadj, idel, nullptr);
+	for (uint64_t i = 0; i < nd; i++) {
+		for (int d = 0; d < 2; d++) {
+			Csr& c = d == 0 ? g->out : g->in;
+			int64_t x = d == 0 ? oe[i] : ie[i];
+			uint64_t& v = c.et[edge_level(x)][edge_index(x)];
+			if ((uint64_t)level < value_max_level(v))
+				v = value_create_ext(value_payload(v), (uint64_t)level);
+		}
+	}
+	return 0;
+}
+
+// Level arrays, for byte comparison with other builders.
+int lgo_level_arrays(void* gp, int dir, int level, const void** vt,
+		uint64_t* n_vt, const uint64_t** et, uint64_t* n_et) {
+	Graph* g = (Graph*)gp;
+	Csr& c = dir == 0 ? g->out : g->in;
+	if (level < 0 || level >= (int)c.vt.size()) return -1;
+	*vt = c.vt[level].data();
+	*n_vt = c.vt[level].size();
+	*et = c.et[level].data();
+	*n_et = c.et[level].size();
+	return 0;
+}
+
+// Adjacency of snapshot `level` in iteration order.  offsets: V+1 entries;
+// nbr / ids may be NULL (then only offsets are written).  Returns #edges.
+uint64_t lgo_adjacency(void* gp, int dir, int level, uint64_t* offsets,
+		uint32_t* nbr, int64_t* ids) {
+	Graph* g = (Graph*)gp;
+	Csr& c = dir == 0 ? g->out : g->in;
+	std::vector<uint32_t> nb;
+	std::vector<int64_t> id;
+	uint64_t o = 0;
+	for (uint64_t v = 0; v < g->V; v++) {
+		offsets[v] = o;
+		neighbours(c, level, v, nb, &id);
+		for (size_t k = 0; k < nb.size(); k++, o++) {
+			if (nbr) nbr[o] = nb[k];
+			if (ids) ids[o] = id[k];
+		}
+	}
+	offsets[g->V] = o;
+	return o;
+}
+
+// Out-degree (dir 0) or in-degree (dir 1): degree(n) with
+// LL_PRECOMPUTED_DEGREE, ll_mlcsr_sp.h:1900-1930.
+void lgo_degrees(void* gp, int dir, int level, uint32_t* deg) {
+	Graph* g = (Graph*)gp;
+	Csr& c = dir == 0 ? g->out : g->in;
+	for (uint64_t v = 0; v < g->V; v++) deg[v] = c.vt[level][v].degree;
+}
+
+// PageRank pull, FP64: ll_b_pagerank_pull_ext::run, pagerank.h:98-182.
+void lgo_pagerank_pull(void* gp, int level, int max, double d, double* rank) {
+	Graph* g = (Graph*)gp;
+	const uint64_t V = g->V;
+	const double N = (double)V;
+	std::vector<double> nxt(V);
+	for (uint64_t t = 0; t < V; t++) rank[t] = 1 / N;
+	std::vector<uint32_t> nb;
+	int cnt = 0;
+	do {
+		for (uint64_t t = 0; t < V; t++) {
+			double S = 0.0;
+			neighbours(g->in, level, t, nb, nullptr);
+			for (uint32_t w : nb)
+				S = S + rank[w] / ((double)g->out.vt[level][w].degree);
+			nxt[t] = (1 - d) / N + d * S;
+		}
+		for (uint64_t t = 0; t < V; t++) rank[t] = nxt[t];
+		cnt = cnt + 1;
+	} while (cnt < max);
+}
+
+// BFS levels: u_sssp_bfs (sssp.h:219-244) / ll_b_sssp_unweighted_bfs::run
+// (sssp.h:285-300): dist = INT_MAX-1, dist[root] = 0, level-synchronous BFS
+// over out-edges.  Returns the number of reached vertices.
+uint64_t lgo_bfs(void* gp, int level, int64_t root, int32_t* dist) {
+	Graph* g = (Graph*)gp;
+	for (uint64_t v = 0; v < g->V; v++) dist[v] = UNREACHED;
+	dist[root] = 0;
+	std::vector<uint32_t> frontier(1, (uint32_t)root), next, nb;
+	uint64_t reached = 1;
+	int32_t cur = 0;
+	while (!frontier.empty()) {
+		next.clear();
+		for (uint32_t u : frontier) {
+			neighbours(g->out, level, u, nb, nullptr);
+			for (uint32_t v : nb)
+				if (dist[v] == UNREACHED) { dist[v] = cur + 1; next.push_back(v); }
+		}
+		reached += next.size();
+		frontier.swap(next);
+		cur++;
+	}
+	return reached;
+}
+
+} // extern "C"

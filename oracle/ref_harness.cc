@@ -1,0 +1,244 @@
+// ref_harness.cc - drives the REFERENCE's own code, compiled from its source
+// tree, for the test suite and the CPU baseline.
+//
+// TEST INFRASTRUCTURE ONLY (see oracle/Makefile).  It includes goatdb/llama's
+// headers (-I <reference>/llama/include -I <reference>/benchmark), builds
+// levels through the reference's public CSR API - ll_mlcsr_core::init_level,
+// init_node, finish_level_vertices, write_value, finish_level_edges and
+// update_max_visible_level_lower_only (llama/include/llama/ll_mlcsr_sp.h:
+// 624-863, 1375-1627) - and runs the reference benchmark kernels over
+// snapshot views ll_mlcsr_ro_graph(master, level)
+// (llama/include/llama/ll_mlcsr_graph.h:318-394).
+//
+// Level sizing: init_level_from_degrees (ll_mlcsr_sp.h:1562-1607) reserves
+// continuation space only for vertices with new edges, while init_node also
+// writes one for vertices that only lose edges (ll_mlcsr_sp.h:1474-1497),
+// which overruns the edge table.  The harness therefore performs the same
+// three calls itself (init_level, init_node per vertex,
+// finish_level_vertices) and counts every vertex with new or deleted edges.
+// No reference source is modified.
+
+#include <llama.h>
+
+#include <time.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "benchmarks/bfs.h"
+#include "benchmarks/sssp.h"
+#include "benchmarks/pagerank.h"
+
+// The per-vertex result arrays of the benchmark classes are private members.
+// An explicit template instantiation may name a private member (C++ [temp.
+// explicit]), which lets the harness read the results without editing the
+// reference: Reader<Tag, &Class::member> defines get(Tag) returning the
+// member pointer.
+template <class Tag, typename Tag::type M>
+struct Reader { friend typename Tag::type get(Tag) { return M; } };
+
+struct PrRankTag {
+	typedef double* ll_b_pagerank_pull_ext<ll_mlcsr_ro_graph, double>::*type;
+	friend type get(PrRankTag);
+};
+template struct Reader<PrRankTag,
+	&ll_b_pagerank_pull_ext<ll_mlcsr_ro_graph, double>::G_pg_rank>;
+
+namespace {
+
+struct RefGraph {
+	uint64_t V;
+	ll_mlcsr_ro_graph* G;
+};
+
+double now_s() {
+	struct timespec ts;
+	clock_gettime(CLOCK_MONOTONIC, &ts);
+	return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+void build_csr_level(LL_CSR& c, uint64_t V, const std::vector<uint32_t>& cnt_new,
+		const std::vector<uint32_t>& cnt_del, int level) {
+	size_t max_edges = 0, adj = 0;
+	for (uint64_t v = 0; v < V; v++) {
+		max_edges += cnt_new[v];
+		if (cnt_new[v] > 0 || (level > 0 && cnt_del[v] > 0)) adj++;
+	}
+	c.init_level(V, adj, max_edges);
+	for (uint64_t v = 0; v < V; v++)
+		c.init_node(v, cnt_new[v], level == 0 ? 0 : cnt_del[v]);
+	c.finish_level_vertices();
+}
+
+} // namespace
+
+extern "C" {
+
+void* llref_create(uint64_t V) {
+	RefGraph* g = new RefGraph();
+	g->V = V;
+	g->G = new ll_mlcsr_ro_graph((ll_database*)NULL);
+	return g;
+}
+
+void llref_destroy(void* gp) {
+	RefGraph* g = (RefGraph*)gp;
+	delete g->G;
+	delete g;
+}
+
+int llref_num_levels(void* gp) { return (int)((RefGraph*)gp)->G->num_levels(); }
+
+// Append a level built from new edges (sorted by (src, dst)) and deletions of
+// edges live in the latest snapshot.
+int llref_add_level(void* gp, const uint32_t* src, const uint32_t* dst,
+		uint64_t n, const uint32_t* dsrc, const uint32_t* ddst, uint64_t nd) {
+	RefGraph* g = (RefGraph*)gp;
+	ll_mlcsr_ro_graph& G = *g->G;
+	const uint64_t V = g->V;
+	const int level = (int)G.num_levels();
+	for (uint64_t i = 1; i < n; i++)
+		if (src[i] < src[i - 1] || (src[i] == src[i - 1] && dst[i] <= dst[i - 1]))
+			return -1;
+	std::vector<int64_t> oe(nd), ie(nd);
+	std::vector<uint32_t> onew(V, 0), inew(V, 0), odel(V, 0), idel(V, 0);
+	for (uint64_t i = 0; i < nd; i++) {
+		if (level == 0) return -1;
+		oe[i] = G.out().find(dsrc[i], ddst[i]);
+		ie[i] = G.in().find(ddst[i], dsrc[i]);
+		if (oe[i] == LL_NIL_EDGE || ie[i] == LL_NIL_EDGE) return -2;
+		odel[dsrc[i]]++;
+		idel[ddst[i]]++;
+	}
+	for (uint64_t i = 0; i < n; i++) { onew[src[i]]++; inew[dst[i]]++; }
+
+	build_csr_level(G.out(), V, onew, odel, level);
+	{
+		std::vector<uint32_t> k(V, 0);
+		for (uint64_t i = 0; i < n; i++)
+			G.out().write_value(src[i], k[src[i]]++, (node_t)dst[i]);
+	}
+	G.out().finish_level_edges();
+
+	// in-edges grouped by target, sources ascending
+	build_csr_level(G.in(), V, inew, idel, level);
+	{
+		std::vector<uint64_t> order(n);
+		for (uint64_t i = 0; i < n; i++) order[i] = i;
+		std::stable_sort(order.begin(), order.end(),
+				[&](uint64_t a, uint64_t b) { return dst[a] < dst[b]; });
+		std::vector<uint32_t> k(V, 0);
+		for (uint64_t j = 0; j < n; j++) {
+			uint64_t i = order[j];
+			G.in().write_value(dst[i], k[dst[i]]++, (node_t)src[i]);
+		}
+	}
+	G.in().finish_level_edges();
+
+	for (uint64_t i = 0; i < nd; i++) {
+		G.out().update_max_visible_level_lower_only(oe[i], level);
+		G.in().update_max_visible_level_lower_only(ie[i], level);
+	}
+	return 0;
+}
+
+// Copy one level's vertex table (V+1 elements of 16 bytes) and its used edge
+// table slots into caller buffers.  With vt == NULL / et == NULL only the
+// slot count is returned.
+int64_t llref_level_arrays(void* gp, int dir, int level, void* vt, uint64_t* et) {
+	RefGraph* g = (RefGraph*)gp;
+	LL_CSR& c = dir == 0 ? g->G->out() : g->G->in();
+	if (level < 0 || level >= (int)c.num_levels()) return -1;
+	uint64_t n_et = c.max_edges(level);
+	if (vt) {
+		auto* t = c.vertex_table(level);
+		for (uint64_t v = 0; v <= g->V; v++) {
+			const ll_mlcsr_core__begin_t& e = (*t)[v];
+			memcpy((char*)vt + 16 * v, &e, 16);
+		}
+	}
+	if (et) {
+		auto* t = c.edge_table(level);
+		for (uint64_t i = 0; i < n_et; i++) et[i] = (*t)[i];
+	}
+	return (int64_t)n_et;
+}
+
+// Neighbours of every vertex in snapshot `level`, in the reference's
+// iteration order (ll_foreach_out / ll_foreach_in).
+uint64_t llref_adjacency(void* gp, int dir, int level, uint64_t* off,
+		uint32_t* nbr) {
+	RefGraph* g = (RefGraph*)gp;
+	ll_mlcsr_ro_graph S(g->G, level);
+	uint64_t o = 0;
+	for (uint64_t v = 0; v < g->V; v++) {
+		off[v] = o;
+		ll_edge_iterator it;
+		if (dir == 0) {
+			S.out_iter_begin(it, v);
+			for (edge_t e = S.out_iter_next(it); e != LL_NIL_EDGE; e = S.out_iter_next(it)) {
+				if (nbr) nbr[o] = (uint32_t)it.last_node;
+				o++;
+			}
+		} else {
+			S.inm_iter_begin(it, v);
+			for (node_t w = S.inm_iter_next(it); w != LL_NIL_NODE; w = S.inm_iter_next(it)) {
+				if (nbr) nbr[o] = (uint32_t)w;
+				o++;
+			}
+		}
+	}
+	off[g->V] = o;
+	return o;
+}
+
+void llref_degrees(void* gp, int level, uint32_t* deg) {
+	RefGraph* g = (RefGraph*)gp;
+	ll_mlcsr_ro_graph S(g->G, level);
+	for (uint64_t v = 0; v < g->V; v++) deg[v] = (uint32_t)S.out_degree(v);
+}
+
+void llref_set_threads(int n) { if (n > 0) omp_set_num_threads(n); }
+int llref_max_threads(void) { return omp_get_max_threads(); }
+
+// "pagerank_double" (benchmark.cc:936-938): returns run() seconds.
+double llref_pagerank(void* gp, int level, int iters, double d, double* out) {
+	RefGraph* g = (RefGraph*)gp;
+	ll_mlcsr_ro_graph S(g->G, level);
+	ll_b_pagerank_pull_double<ll_mlcsr_ro_graph> b(iters, d);
+	b.initialize(&S);
+	double t0 = now_s();
+	b.run();
+	double t = now_s() - t0;
+	if (out) memcpy(out, b.*get(PrRankTag()), sizeof(double) * g->V);
+	b.finalize();
+	return t;
+}
+
+// "sssp_unweighted" levels via u_sssp_bfs (sssp.h:219-300): returns seconds.
+double llref_bfs_levels(void* gp, int level, int64_t root, int32_t* dist) {
+	RefGraph* g = (RefGraph*)gp;
+	ll_mlcsr_ro_graph S(g->G, level);
+	for (uint64_t v = 0; v < g->V; v++) dist[v] = INT_MAX - 1;
+	node_t r = root;
+	dist[r] = 0;
+	double t0 = now_s();
+	u_sssp_bfs<ll_mlcsr_ro_graph> bfs(S, r, dist);
+	bfs.prepare(r);
+	bfs.do_bfs_forward();
+	return now_s() - t0;
+}
+
+// "bfs_count" (bfs.h:117-127): returns the count; *secs = run() seconds.
+double llref_bfs_count(void* gp, int level, int64_t root, double* secs) {
+	RefGraph* g = (RefGraph*)gp;
+	ll_mlcsr_ro_graph S(g->G, level);
+	ll_b_bfs<ll_mlcsr_ro_graph> b(root);
+	b.initialize(&S);
+	double t0 = now_s();
+	double r = b.run();
+	if (secs) *secs = now_s() - t0;
+	return r;
+}
+
+} // extern "C"
