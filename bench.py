@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""Benchmark: PageRank pull + BFS GTEPS over a multiversion R-MAT store.
+
+Workload (default): directed R-MAT scale 24 (2^24 vertices, 16 * 2^24 draws,
+a/b/c/d = .57/.19/.19/.05, self-loops and duplicates removed, seed 2), split
+into 8 levels: a seeded 90 % of the edges form level 0, levels 1..7 each add
+~1.4 % and delete 0.2 % of the live edges (deletion marks in older levels).
+One step on the latest snapshot = FP64 PageRank pull, 20 iterations, d = 0.85
++ BFS from 16 roots (seed 3, out-degree > 0).
+
+value    = traversed edges per second of the device-resident step:
+           (20 * E_live + sum over roots of E_reach) / step time  [GTEPS]
+e2e      = the same step through the C ABI with host buffers: every step
+           re-ingests the newest level from host memory (pinned staging),
+           reopens the snapshot and copies ranks and BFS levels back to host
+roofline = the PageRank iteration kernel (pr_pull_step), HBM-bound
+--impl reference times the reference's own OpenMP kernels (oracle/_ref, built
+from the reference source) on the host cores for the same step.
+
+N > 1 (torchrun): independent replicas, one store per GPU (the path does not
+shard), weak scaling; value = all ranks' edges / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GTEPS (PageRank iter, BFS) on multiversion R-MAT; batched BC & adjoint vs plain"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="lg", choices=["lg", "reference"])
+    p.add_argument("--scale", type=int, default=24)
+    p.add_argument("--levels", type=int, default=8)
+    p.add_argument("--pr-iters", type=int, default=20)
+    p.add_argument("--roots", type=int, default=16)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--out", default=None, help="also write the JSON line here")
+    return p.parse_args()
+
+
+def workload(args):
+    from llama_b200 import workloads
+    spec = workloads.rmat_multiversion(scale=args.scale, seed=2, levels=args.levels,
+                                       level0=0.90, delete=0.002)
+    cfg = {"workload": f"rmat{args.scale}_{args.levels}level_del0.2pct",
+           "graph": f"directed R-MAT scale {args.scale}, edge factor 16, "
+                    f"{args.levels} levels (90% in level 0, 0.2% deletions per level)",
+           "step": f"PageRank pull FP64 x{args.pr_iters} iterations + BFS from "
+                   f"{args.roots} roots, latest snapshot",
+           "pr_iterations": args.pr_iters, "damping": 0.85, "bfs_roots": args.roots}
+    return spec, cfg
+
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        backend = "nccl" if args.impl == "lg" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        rows = []
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                rows.append((float(f[0]), float(f[1]), f[4], f[5], f[6], f[7]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        reasons = set()
+        for r in rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown",
+                                "sw_thermal_slowdown", "sw_power_cap"), r[2:]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r[0] for r in rows),
+                "sm_max_mhz": max(r[1] for r in rows), "samples": len(rows),
+                "reasons": sorted(reasons)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per pr_pull_step launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "pr_pull_step_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def run_reference(args):
+    ws, rank, local = dist_init(args)
+    if rank != 0:
+        return
+    from llama_b200 import HostGraph
+    from oracle.bind import Reference, ref_available
+    spec, cfg = workload(args)
+    if not ref_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libllref.so was not built"}))
+        return
+    hg = HostGraph.from_spec(spec)
+    R = Reference(spec.max_nodes)
+    for l in range(hg.num_levels):
+        R.add_level(*hg.level_input(l)[:4])
+    del hg
+    from llama_b200 import workloads
+    deg = R.degrees(-1)
+    roots = workloads.pick_roots(deg, args.roots, seed=3)
+    E = int(deg.sum())
+    cores = Reference.max_threads()
+
+    def step():
+        pr, t_pr = R.pagerank_pull(-1, args.pr_iters, 0.85)
+        edges, t_bfs = 0, 0.0
+        for r in roots:
+            lv, t = R.bfs(-1, int(r))
+            t_bfs += t
+            edges += int(deg[lv < 2147483646].sum(dtype=np.int64))
+        return t_pr + t_bfs, args.pr_iters * E + edges
+
+    for _ in range(args.warmup):
+        step()
+    tot_t, tot_e = 0.0, 0
+    for _ in range(args.steps):
+        t, e = step()
+        tot_t += t
+        tot_e += e
+    gteps = tot_e / tot_t / 1e9
+    line = {"metric": METRIC, "value": gteps, "unit": "GTEPS", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * tot_t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": cfg,
+            "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": cores,
+                             "kind": "reference",
+                             "sample": "each step = the full step (pagerank_double x"
+                                       f"{args.pr_iters} + sssp_unweighted BFS from "
+                                       f"{len(roots)} roots) on the same store, run() "
+                                       "time only"},
+            "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    emit(line, args)
+
+
+def emit(line, args):
+    s = json.dumps(line)
+    print(s, flush=True)
+    if args.out:
+        with open(args.out, "w") as f:
+            f.write(s + "\n")
+
+
+def run_lg(args):
+    import torch
+    ws, rank, local = dist_init(args)
+    torch.cuda.set_device(local)
+    from llama_b200 import HostGraph, Store, workloads
+    spec, cfg = workload(args)
+    cfg["parallelism"] = f"replicas{ws}"
+    t0 = time.time()
+    hg = HostGraph.from_spec(spec)
+    build_s = time.time() - t0
+
+    stream = torch.cuda.Stream(device=local)
+    st = Store(device=local, stream=stream.cuda_stream)
+    t0 = time.time()
+    st.ingest(hg)
+    ingest_s = time.time() - t0
+    sn = st.snapshot()
+    V = sn.max_nodes
+    deg = sn.out_degrees()
+    roots = workloads.pick_roots(deg, args.roots, seed=3)
+    E = sn.num_edges
+    ins = sn.stats(1)
+
+    pr_dev = torch.empty(V, dtype=torch.float64, device=f"cuda:{local}")
+    lv_dev = torch.empty((len(roots), V), dtype=torch.int32, device=f"cuda:{local}")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+
+    def step():
+        ev[0].record(stream)
+        sn.pagerank_pull(args.pr_iters, 0.85, out=pr_dev)
+        ev[1].record(stream)
+        reach = 0
+        for i, r in enumerate(roots):
+            _, res = sn.bfs(int(r), out=lv_dev[i])
+            reach += res.reach_edges
+        ev[2].record(stream)
+        return reach
+
+    for _ in range(max(3, args.warmup)):
+        reach = step()
+    st.sync()
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    launches0 = st.launch_count
+    pr_ms, bfs_ms, edges = 0.0, 0.0, 0
+    t_start.record(stream)
+    for _ in range(args.steps):
+        reach = step()
+        stream.synchronize()
+        pr_ms += ev[0].elapsed_time(ev[1])
+        bfs_ms += ev[1].elapsed_time(ev[2])
+        edges += args.pr_iters * E + reach
+    t_end.record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = st.launch_count - launches0
+    ms = t_start.elapsed_time(t_end)
+    ms_max, edges_all = reduce_max_sum(ws, ms, edges)
+    value = edges_all / (ms_max / 1e3) / 1e9
+
+    # roofline of the PageRank iteration kernel (in-CSR of the snapshot)
+    pr_bytes = (ins["live_edges"] * (4 + 8) + ins["slots"] / 8 + ins["fragments"] * 12
+                + V * (8 + 8 + 4))
+    launch_s = pr_ms / 1e3 / (args.steps * args.pr_iters)
+    peak, peak_kind = measured_peak()
+    achieved = pr_bytes / launch_s / 1e9
+    traffic = profiled_traffic()
+    roofline = {"bound": "hbm", "kernel": "pr_pull_step", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                               if peak_kind == "measured" else "fallback 6.65 TB/s",
+                "algorithmic_bytes_per_launch": pr_bytes,
+                "launch_ms": launch_s * 1e3,
+                "traffic": traffic["dram_bytes_per_launch_scaled"] if traffic else None}
+
+    # e2e: newest level re-ingested from host, snapshot reopened, results to host
+    e2e = None
+    if not args.no_e2e:
+        sn.close()
+        pr_host = torch.empty(V, dtype=torch.float64).pin_memory()
+        lv_host = torch.empty((len(roots), V), dtype=torch.int32).pin_memory()
+        L = hg.num_levels - 1
+        desc = hg.level_desc(L)
+
+        def e2e_step():
+            st.drop_level()
+            st.ingest_level(desc)
+            s2 = st.snapshot()
+            s2.pagerank_pull(args.pr_iters, 0.85, out=pr_host)
+            reach = 0
+            for i, r in enumerate(roots):
+                _, res = s2.bfs(int(r), out=lv_host[i])
+                reach += res.reach_edges
+            s2.close()
+            return reach
+        e2e_step()
+        st.sync()
+        barrier(ws)
+        h0, d0 = st.transfer_bytes()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e2e_edges = 0
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_edges += args.pr_iters * E + e2e_step()
+        e1.record(stream)
+        stream.synchronize()
+        h1, d1 = st.transfer_bytes()
+        e2e_ms = e0.elapsed_time(e1)
+        e2e_ms_max, e2e_edges_all = reduce_max_sum(ws, e2e_ms, e2e_edges)
+        e2e = {"value": e2e_edges_all / (e2e_ms_max / 1e3) / 1e9, "unit": "GTEPS",
+               "h2d_bytes_per_step": (h1 - h0) // args.steps,
+               "d2h_bytes_per_step": (d1 - d0) // args.steps,
+               "ms_per_step": e2e_ms_max / args.steps,
+               "includes": "ingest of the newest level from host + snapshot open + "
+                           "PageRank + BFS with results copied to pinned host memory"}
+        sn = None
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(hg, spec, roots, args)
+
+    line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": ws,
+            "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded R-MAT generator, no dataset)",
+            "config": dict(cfg, l2="inputs larger than L2: store %.1f GB on the device"
+                           % (st.device_bytes / 1e9)),
+            "kernels": {"pagerank_pull": {"ms_per_step": pr_ms / args.steps,
+                                          "gteps": args.pr_iters * E * args.steps / (pr_ms / 1e3) / 1e9},
+                        "bfs": {"ms_per_step": bfs_ms / args.steps,
+                                "gteps": (edges - args.pr_iters * E * args.steps)
+                                / (bfs_ms / 1e3) / 1e9, "last_reach_edges": reach}},
+            "graph": {"max_nodes": V, "live_edges": E, "in_slots": ins["slots"],
+                      "in_fragments": ins["fragments"], "levels": hg.num_levels,
+                      "host_build_s": build_s, "ingest_s": ingest_s},
+            "roofline": roofline, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk, "cpu_baseline": cpu}
+    if rank == 0:
+        emit(line, args)
+    if sn is not None:
+        sn.close()
+    st.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(hg, spec, roots, args):
+    """Reference OpenMP kernels on this host's cores, one step (bounded)."""
+    from oracle.bind import Reference, ref_available
+    if not ref_available():
+        return None
+    t0 = time.time()
+    R = Reference(spec.max_nodes)
+    for l in range(hg.num_levels):
+        R.add_level(*hg.level_input(l)[:4])
+    build_s = time.time() - t0
+    deg = R.degrees(-1)
+    E = int(deg.sum())
+    _, t_pr = R.pagerank_pull(-1, args.pr_iters, 0.85)
+    t_bfs, reach = 0.0, 0
+    for r in roots:
+        lv, t = R.bfs(-1, int(r))
+        t_bfs += t
+        reach += int(deg[lv < 2147483646].sum(dtype=np.int64))
+    gteps = (args.pr_iters * E + reach) / (t_pr + t_bfs) / 1e9
+    return {"value": gteps, "unit": "GTEPS", "cores": Reference.max_threads(),
+            "kind": "reference",
+            "sample": f"one full step (pagerank_double x{args.pr_iters} + sssp_unweighted "
+                      f"BFS from {len(roots)} roots) on the same store, run() time only",
+            "pagerank_s": t_pr, "bfs_s": t_bfs, "store_build_s": build_s}
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reduce_max_sum(ws, ms, edges):
+    if ws == 1:
+        return ms, edges
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    e = torch.tensor([float(edges)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(e.item())
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_lg(args)
+
+
+if __name__ == "__main__":
+    main()

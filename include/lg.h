@@ -159,8 +159,20 @@ lg_status lg_store_max_nodes(const lg_store* store, int level, uint64_t* max_nod
 lg_status lg_store_sync(lg_store* store);
 /* The stream every call of this store runs on (a cudaStream_t). */
 void*     lg_store_stream(const lg_store* store);
-/* Device bytes held by the store (levels, deletions, snapshots). */
+/* Device bytes held by the store (levels, deletions, scratch). */
 uint64_t  lg_store_device_bytes(const lg_store* store);
+/* Number of kernels this store has launched so far (all calls). */
+uint64_t  lg_store_launch_count(const lg_store* store);
+/* Bytes this store has copied host -> device and device -> host so far
+ * (level ingest, deletion lists, results copied to host buffers, and the
+ * per-step counters iterative kernels report). */
+lg_status lg_store_transfer_bytes(const lg_store* store, uint64_t* h2d,
+		uint64_t* d2h);
+/* Remove the latest level and the deletion marks it made in older levels,
+ * restoring the store to the state before its ingest (the inverse of
+ * lg_store_ingest_level; used to age out or re-ingest a snapshot).  Fails with
+ * LG_ESTATE while snapshots are open. */
+lg_status lg_store_drop_level(lg_store* store);
 
 /* ---------------------------------------------------------------------------
  * Snapshots.  A read-only view whose latest level is `level`, with deletions
@@ -178,6 +190,20 @@ lg_status lg_snapshot_level(const lg_snapshot* snap, int* level);
 lg_status lg_snapshot_max_nodes(const lg_snapshot* snap, uint64_t* max_nodes);
 /* Number of live edges (sum of out-degrees) of the snapshot. */
 lg_status lg_snapshot_num_edges(const lg_snapshot* snap, uint64_t* num_edges);
+
+/* Sizes of one direction (0 out, 1 in) of a snapshot, for byte models. */
+typedef struct lg_snapshot_stats {
+	uint64_t max_nodes;
+	uint64_t live_edges;    /* sum of live degrees                        */
+	uint64_t slots;         /* edge-table slots of levels 0..L, continuation
+	                           records included                           */
+	uint64_t fragment_slots;/* slots covered by the vertices' fragments   */
+	uint64_t fragments;     /* (vertex, level) fragments                  */
+	uint64_t hubs;          /* vertices reduced by whole CTAs             */
+	uint64_t deletions;     /* deletion marks visible in the snapshot     */
+} lg_snapshot_stats;
+lg_status lg_snapshot_get_stats(const lg_snapshot* snap, int dir,
+		lg_snapshot_stats* stats);
 
 /* Live out-degree per vertex, uint32[max_nodes]:
  * ll_mlcsr_ro_graph::out_degree (llama/include/llama/ll_mlcsr_graph.h:726-741). */

@@ -68,6 +68,13 @@ class lg_bfs_result(C.Structure):
                 ("bottom_up_steps", C.c_int32), ("reserved", C.c_int32)]
 
 
+class lg_snapshot_stats(C.Structure):
+    _fields_ = [("max_nodes", C.c_uint64), ("live_edges", C.c_uint64),
+                ("slots", C.c_uint64), ("fragment_slots", C.c_uint64),
+                ("fragments", C.c_uint64), ("hubs", C.c_uint64),
+                ("deletions", C.c_uint64)]
+
+
 class lg_graph_spec(C.Structure):
     _fields_ = [("kind", C.c_int), ("scale", C.c_int), ("edge_factor", C.c_double),
                 ("a", C.c_double), ("b", C.c_double), ("c", C.c_double),
@@ -95,6 +102,10 @@ SIGNATURES = [
     ("lg_store_sync", _INT, [_P]),
     ("lg_store_stream", _P, [_P]),
     ("lg_store_device_bytes", _U64, [_P]),
+    ("lg_store_launch_count", _U64, [_P]),
+    ("lg_store_transfer_bytes", _INT, [_P, C.POINTER(_U64), C.POINTER(_U64)]),
+    ("lg_store_drop_level", _INT, [_P]),
+    ("lg_snapshot_get_stats", _INT, [_P, _INT, C.POINTER(lg_snapshot_stats)]),
     ("lg_snapshot_open", _INT, [_P, _INT, _PP]),
     ("lg_snapshot_close", _INT, [_P]),
     ("lg_snapshot_level", _INT, [_P, C.POINTER(_INT)]),

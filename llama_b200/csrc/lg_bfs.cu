@@ -135,6 +135,7 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 
 	bfs_init<<<grid_for(V, 256), 256, 0, st>>>(lvl, V, (uint32_t)root, q, outdeg, ctr);
 	LG_CUDA(cudaGetLastError(), "bfs_init");
+	s->launches++;
 	unsigned long long h[2];
 	LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
 	LG_CUDA(cudaStreamSynchronize(st), "bfs");
@@ -156,15 +157,18 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 			bfs_top_down<<<grid_for(warps, kBfsThreads / 32), kBfsThreads, 0, st>>>(
 					out, q, (uint32_t)qlen, lvl, nq, ctr, cur);
 			td_steps++;
+			s->launches++;
 		} else {
 			LG_CUDA(cudaMemsetAsync(bits, 0, ((V + 31) / 32) * 4, st), "memset");
 			bfs_set_bits<<<grid_for(qlen, 256), 256, 0, st>>>(q, (uint32_t)qlen, bits);
 			bfs_bottom_up<<<grid_for(V, kBfsThreads), kBfsThreads, 0, st>>>(
 					in, outdeg, bits, lvl, nq, ctr, cur);
 			bu_steps++;
+			s->launches += 2;
 		}
 		LG_CUDA(cudaGetLastError(), "bfs step");
 		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+		s->d2h_bytes += sizeof(h);
 		LG_CUDA(cudaStreamSynchronize(st), "bfs step");
 		qlen = h[0];
 		mf = h[1];
@@ -175,7 +179,7 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 		cur++;
 	}
 	if (!dev_out) {
-		LG_TRY(copy_out(levels, lvl, V * 4, st));
+		LG_TRY(copy_out(s, levels, lvl, V * 4));
 		LG_CUDA(cudaStreamSynchronize(st), "bfs");
 	}
 	if (result) {

@@ -161,6 +161,7 @@ struct DevLevel {
 struct DevCsr {
 	std::vector<DevLevel*> levels;
 	std::vector<uint2> dels_host;   // (index, level << 26 | max_visible_level)
+	std::vector<size_t> dels_mark;  // dels_host.size() before each level's ingest
 	DevBuf dels;                    // device copy of dels_host
 	uint64_t n_dels_dev = 0;
 	~DevCsr() { for (DevLevel* l : levels) delete l; }
@@ -170,6 +171,9 @@ struct SnapDir {
 	DevBuf frag_off, frags, deg, delbits, lt, hubs, hub_chunk_off;
 	uint64_t n_frags = 0;
 	uint64_t n_edges = 0;          // live edges (sum of degrees)
+	uint64_t n_slots = 0;          // slots of levels 0..L
+	uint64_t n_frag_slots = 0;     // slots covered by fragments
+	uint64_t n_dels = 0;           // deletion marks visible at L
 	uint32_t n_hubs = 0;
 	uint32_t n_hub_chunks = 0;
 	bool present = false;
@@ -199,6 +203,9 @@ struct lg_store {
 	// scratch shared by the analytics calls of this store
 	lg::DevBuf scratch[8];
 	int open_snapshots = 0;
+	uint64_t launches = 0;      // kernels launched by this store
+	uint64_t h2d_bytes = 0;     // host -> device bytes copied by this store
+	uint64_t d2h_bytes = 0;     // device -> host bytes copied by this store
 };
 
 struct lg_snapshot {
@@ -229,8 +236,9 @@ bool is_device_pointer(const void* p);
 lg_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n,
 		DevBuf& tmp, cudaStream_t stream, uint64_t* total);
 
-// Copy `bytes` of device data to a caller buffer (host or device).
-lg_status copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s);
+// Copy `bytes` of device data to a caller buffer (host or device) on the
+// store's stream, counting host-bound bytes.
+lg_status copy_out(lg_store* s, void* dst, const void* src, size_t bytes);
 
 inline unsigned grid_for(uint64_t n, unsigned block) {
 	uint64_t g = (n + block - 1) / block;

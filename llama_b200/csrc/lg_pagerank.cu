@@ -191,6 +191,7 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 	pr_init<<<grid_for(V, 256), 256, 0, st>>>(sn->out.deg.as<uint32_t>(), V, pr0,
 			sc[0].as<double>(), iterations == 0 ? pr_buf : nullptr);
 	LG_CUDA(cudaGetLastError(), "pr_init");
+	s->launches++;
 
 	PrArgs a;
 	a.in = sn->view(1);
@@ -213,8 +214,9 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 		pr_pull_step<<<(unsigned)grid, kPrThreads, 0, st>>>(a);
 	}
 	LG_CUDA(cudaGetLastError(), "pr_pull_step");
+	s->launches += iterations;
 	if (!dev_out) {
-		LG_TRY(copy_out(ranks, pr_buf, V * sizeof(double), st));
+		LG_TRY(copy_out(s, ranks, pr_buf, V * sizeof(double)));
 		LG_CUDA(cudaStreamSynchronize(st), "pagerank");
 	}
 	return LG_OK;

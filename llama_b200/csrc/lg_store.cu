@@ -57,9 +57,10 @@ bool is_device_pointer(const void* ptr) {
 	return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
-lg_status copy_out(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+lg_status copy_out(lg_store* s, void* dst, const void* src, size_t bytes) {
 	if (bytes == 0) return LG_OK;
-	LG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s), "copy result");
+	if (!is_device_pointer(dst)) s->d2h_bytes += bytes;
+	LG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s->stream), "copy result");
 	return LG_OK;
 }
 
@@ -203,6 +204,7 @@ static lg_status staged_copy(lg_store* s, void* dst, size_t bytes, Fill&& fill) 
 		LG_CUDA(cudaMemcpyAsync((char*)dst + off, st, n,
 				cudaMemcpyHostToDevice, s->stream), "ingest copy");
 		LG_CUDA(cudaEventRecord(s->staged[half], s->stream), "staging event");
+		s->h2d_bytes += n;
 		off += n;
 		half ^= 1;
 	}
@@ -324,6 +326,7 @@ static lg_status ingest_csr(lg_store* s, DevCsr& csr, int l,
 		}
 		add.push_back(make_uint2((uint32_t)ix, (el << LG_BITS_LEVEL) | x.max_visible_level));
 	}
+	csr.dels_mark.push_back(csr.dels_host.size());
 	csr.levels.push_back(d);
 	csr.dels_host.insert(csr.dels_host.end(), add.begin(), add.end());
 	if (!csr.dels_host.empty()) {
@@ -335,6 +338,7 @@ static lg_status ingest_csr(lg_store* s, DevCsr& csr, int l,
 		}
 		LG_CUDA(cudaMemcpyAsync(csr.dels.p, csr.dels_host.data(), need,
 				cudaMemcpyHostToDevice, s->stream), "deletion list");
+		s->h2d_bytes += need;
 		// the host vector must outlive the async copy from pageable memory;
 		// pageable copies complete before cudaMemcpyAsync returns
 		csr.n_dels_dev = csr.dels_host.size();
@@ -433,6 +437,7 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 			cnt.as<uint32_t>(), d.deg.as<uint32_t>(), slots.as<uint32_t>(),
 			nullptr, nullptr);
 	LG_CUDA(cudaGetLastError(), "walk_fragments");
+	s->launches += 5;   // two walks and the three scan kernels
 	uint64_t F = 0;
 	LG_TRY(exclusive_scan_u32(cnt.as<uint32_t>(), d.frag_off.as<uint32_t>(), V,
 			scan_tmp, st, &F));
@@ -468,6 +473,7 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 				csr.dels.as<uint2>(), csr.n_dels_dev, L,
 				(uint32_t* const*)words.p);
 		LG_CUDA(cudaGetLastError(), "mark_deletions");
+		s->launches++;
 		LG_CUDA(cudaStreamSynchronize(st), "snapshot deletions");
 	}
 
@@ -481,12 +487,23 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 			hub_tmp.as<uint32_t>(), (uint32_t*)counters.p, cap);
 	sum_u32<<<592, B, 0, st>>>(d.deg.as<uint32_t>(), V,
 			counters.as<unsigned long long>() + 1);
+	sum_u32<<<592, B, 0, st>>>(slots.as<uint32_t>(), V,
+			counters.as<unsigned long long>() + 2);
 	LG_CUDA(cudaGetLastError(), "hub scan");
-	unsigned long long hc[2];
+	s->launches += 3;
+	unsigned long long hc[3];
 	LG_CUDA(cudaMemcpyAsync(hc, counters.p, sizeof(hc), cudaMemcpyDeviceToHost, st), "d2h");
 	LG_CUDA(cudaStreamSynchronize(st), "hub scan");
 	uint32_t nh = (uint32_t)(hc[0] & 0xffffffffu);
 	d.n_edges = hc[1];
+	d.n_frag_slots = hc[2];
+	d.n_slots = 0;
+	for (int l = 0; l <= L; l++) d.n_slots += csr.levels[l]->n_slots;
+	d.n_dels = 0;
+	for (const uint2& x : csr.dels_host) {
+		uint32_t lv = x.y >> LG_BITS_LEVEL, ml = x.y & ((1u << LG_BITS_LEVEL) - 1u);
+		d.n_dels += ((int)lv <= L && (int)ml <= L);
+	}
 	if (nh > cap) return set_error(LG_ENOTSUP, "too many hub vertices");
 	std::vector<uint32_t> hubs(nh), hub_slots(nh);
 	LG_TRY(d.hubs.reserve(std::max<uint32_t>(nh, 1) * 4));
@@ -498,6 +515,7 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 		gather_u32<<<grid_for(nh, B), B, 0, st>>>(slots.as<uint32_t>(),
 				d.hubs.as<uint32_t>(), nh, hub_tmp.as<uint32_t>());
 		LG_CUDA(cudaGetLastError(), "gather hub slots");
+		s->launches++;
 		LG_CUDA(cudaMemcpyAsync(hub_slots.data(), hub_tmp.p, nh * 4,
 				cudaMemcpyDeviceToHost, st), "d2h");
 		LG_CUDA(cudaStreamSynchronize(st), "hub slots");
@@ -709,6 +727,52 @@ uint64_t lg_store_device_bytes(const lg_store* s) {
 	return b;
 }
 
+uint64_t lg_store_launch_count(const lg_store* s) { return s ? s->launches : 0; }
+
+lg_status lg_store_transfer_bytes(const lg_store* s, uint64_t* h2d, uint64_t* d2h) {
+	clear_error();
+	if (!s) return set_error(LG_EINVAL, "null store");
+	if (h2d) *h2d = s->h2d_bytes;
+	if (d2h) *d2h = s->d2h_bytes;
+	return LG_OK;
+}
+
+lg_status lg_store_drop_level(lg_store* s) {
+	clear_error();
+	if (!s) return set_error(LG_EINVAL, "null store");
+	if (s->out.levels.empty()) return set_error(LG_ESTATE, "the store holds no level");
+	if (s->open_snapshots > 0)
+		return set_error(LG_ESTATE, "close all snapshots before dropping a level");
+	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+	LG_CUDA(cudaStreamSynchronize(s->stream), "drop level");
+	for (DevCsr* c : {&s->out, &s->in}) {
+		if (c->levels.empty()) continue;
+		delete c->levels.back();
+		c->levels.pop_back();
+		// the device copy keeps the same prefix of the list
+		c->dels_host.resize(c->dels_mark.back());
+		c->dels_mark.pop_back();
+		c->n_dels_dev = c->dels_host.size();
+	}
+	return LG_OK;
+}
+
+lg_status lg_snapshot_get_stats(const lg_snapshot* sn, int dir, lg_snapshot_stats* st) {
+	clear_error();
+	if (!sn || !st) return set_error(LG_EINVAL, "null argument");
+	if (dir != 0 && dir != 1) return set_error(LG_EINVAL, "dir must be 0 or 1");
+	const SnapDir& d = dir == 0 ? sn->out : sn->in;
+	if (!d.present) return set_error(LG_ESTATE, "the store has no in-CSR");
+	st->max_nodes = sn->V;
+	st->live_edges = d.n_edges;
+	st->slots = d.n_slots;
+	st->fragment_slots = d.n_frag_slots;
+	st->fragments = d.n_frags;
+	st->hubs = d.n_hubs;
+	st->deletions = d.n_dels;
+	return LG_OK;
+}
+
 lg_status lg_snapshot_open(lg_store* s, int level, lg_snapshot** out) {
 	clear_error();
 	if (!s || !out) return set_error(LG_EINVAL, "null argument");
@@ -765,7 +829,7 @@ static lg_status degrees(lg_snapshot* sn, int dir, uint32_t* out) {
 	if (!d.present) return set_error(LG_ESTATE, "the store has no in-CSR");
 	lg_store* s = sn->store;
 	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
-	LG_TRY(copy_out(out, d.deg.p, sn->V * sizeof(uint32_t), s->stream));
+	LG_TRY(copy_out(s, out, d.deg.p, sn->V * sizeof(uint32_t)));
 	LG_CUDA(cudaStreamSynchronize(s->stream), "degrees");
 	return LG_OK;
 }
@@ -792,6 +856,7 @@ lg_status lg_snapshot_adjacency(lg_snapshot* sn, int dir, uint64_t* offsets,
 	widen_offsets<<<1, 1024, 0, st>>>(cnt.as<uint32_t>(), V,
 			off.as<unsigned long long>());
 	LG_CUDA(cudaGetLastError(), "adjacency offsets");
+	s->launches += 3;
 	uint64_t E = 0;
 	LG_CUDA(cudaMemcpyAsync(&E, off.as<unsigned long long>() + V, 8,
 			cudaMemcpyDeviceToHost, st), "d2h");
@@ -802,9 +867,9 @@ lg_status lg_snapshot_adjacency(lg_snapshot* sn, int dir, uint64_t* offsets,
 			off.as<unsigned long long>(), nb.as<uint32_t>(),
 			edge_ids ? ei.as<long long>() : nullptr);
 	LG_CUDA(cudaGetLastError(), "write_adjacency");
-	LG_TRY(copy_out(offsets, off.p, (V + 1) * 8, st));
-	if (neighbors) LG_TRY(copy_out(neighbors, nb.p, E * 4, st));
-	if (edge_ids) LG_TRY(copy_out(edge_ids, ei.p, E * 8, st));
+	LG_TRY(copy_out(s, offsets, off.p, (V + 1) * 8));
+	if (neighbors) LG_TRY(copy_out(s, neighbors, nb.p, E * 4));
+	if (edge_ids) LG_TRY(copy_out(s, edge_ids, ei.p, E * 8));
 	LG_CUDA(cudaStreamSynchronize(st), "adjacency");
 	return LG_OK;
 }

@@ -172,6 +172,19 @@ class Store:
     def sync(self):
         check(lib.lg_store_sync(self._h))
 
+    @property
+    def launch_count(self):
+        return lib.lg_store_launch_count(self._h)
+
+    def drop_level(self):
+        check(lib.lg_store_drop_level(self._h))
+
+    def transfer_bytes(self):
+        """(host->device, device->host) bytes copied by this store so far."""
+        h, d = C.c_uint64(), C.c_uint64()
+        check(lib.lg_store_transfer_bytes(self._h, C.byref(h), C.byref(d)))
+        return h.value, d.value
+
     def snapshot(self, level=-1):
         return Snapshot(self, level)
 
@@ -210,6 +223,11 @@ class Snapshot:
         n = C.c_uint64()
         check(lib.lg_snapshot_num_edges(self._h, C.byref(n)))
         return n.value
+
+    def stats(self, direction=0):
+        st = _lib.lg_snapshot_stats()
+        check(lib.lg_snapshot_get_stats(self._h, direction, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in st._fields_}
 
     def out_degrees(self):
         out = np.empty(self.max_nodes, np.uint32)

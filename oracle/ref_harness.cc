@@ -70,6 +70,22 @@ void build_csr_level(LL_CSR& c, uint64_t V, const std::vector<uint32_t>& cnt_new
 	c.finish_level_vertices();
 }
 
+// Snapshot to run on.  level < 0 (or the latest level) uses the store itself.
+// An older level uses the reference's view ll_mlcsr_ro_graph(master, level);
+// note that the view copies the master's _maxLevel (ll_mlcsr_sp.h:277), so
+// its iterators filter deletions at the master's latest level, not at
+// `level`.  The test suite therefore pins snapshot L against a store that
+// holds exactly levels 0..L.
+struct View {
+	ll_mlcsr_ro_graph* clone;
+	ll_mlcsr_ro_graph* g;
+	View(RefGraph* r, int level) : clone(NULL), g(r->G) {
+		if (level >= 0 && level < (int)r->G->num_levels() - 1)
+			g = clone = new ll_mlcsr_ro_graph(r->G, level);
+	}
+	~View() { delete clone; }
+};
+
 } // namespace
 
 extern "C" {
@@ -112,26 +128,29 @@ int llref_add_level(void* gp, const uint32_t* src, const uint32_t* dst,
 	}
 	for (uint64_t i = 0; i < n; i++) { onew[src[i]]++; inew[dst[i]]++; }
 
+	// write_value touches only the slots of `node`, so distinct vertices are
+	// written in parallel
+	std::vector<uint64_t> off(V + 1, 0);
 	build_csr_level(G.out(), V, onew, odel, level);
-	{
-		std::vector<uint32_t> k(V, 0);
-		for (uint64_t i = 0; i < n; i++)
-			G.out().write_value(src[i], k[src[i]]++, (node_t)dst[i]);
-	}
+	for (uint64_t v = 0; v < V; v++) off[v + 1] = off[v] + onew[v];
+#pragma omp parallel for schedule(dynamic, 4096)
+	for (uint64_t v = 0; v < V; v++)
+		for (uint64_t k = 0; k < onew[v]; k++)
+			G.out().write_value(v, k, (node_t)dst[off[v] + k]);
 	G.out().finish_level_edges();
 
-	// in-edges grouped by target, sources ascending
+	// in-edges grouped by target, sources ascending (the input is sorted by
+	// source, so a stable counting sort by target keeps them ascending)
 	build_csr_level(G.in(), V, inew, idel, level);
 	{
-		std::vector<uint64_t> order(n);
-		for (uint64_t i = 0; i < n; i++) order[i] = i;
-		std::stable_sort(order.begin(), order.end(),
-				[&](uint64_t a, uint64_t b) { return dst[a] < dst[b]; });
-		std::vector<uint32_t> k(V, 0);
-		for (uint64_t j = 0; j < n; j++) {
-			uint64_t i = order[j];
-			G.in().write_value(dst[i], k[dst[i]]++, (node_t)src[i]);
-		}
+		for (uint64_t v = 0; v < V; v++) off[v + 1] = off[v] + inew[v];
+		std::vector<uint32_t> by_dst(n);
+		std::vector<uint64_t> fill(off.begin(), off.end() - 1);
+		for (uint64_t i = 0; i < n; i++) by_dst[fill[dst[i]]++] = src[i];
+#pragma omp parallel for schedule(dynamic, 4096)
+		for (uint64_t v = 0; v < V; v++)
+			for (uint64_t k = 0; k < inew[v]; k++)
+				G.in().write_value(v, k, (node_t)by_dst[off[v] + k]);
 	}
 	G.in().finish_level_edges();
 
@@ -169,7 +188,8 @@ int64_t llref_level_arrays(void* gp, int dir, int level, void* vt, uint64_t* et)
 uint64_t llref_adjacency(void* gp, int dir, int level, uint64_t* off,
 		uint32_t* nbr) {
 	RefGraph* g = (RefGraph*)gp;
-	ll_mlcsr_ro_graph S(g->G, level);
+	View view(g, level);
+	ll_mlcsr_ro_graph& S = *view.g;
 	uint64_t o = 0;
 	for (uint64_t v = 0; v < g->V; v++) {
 		off[v] = o;
@@ -194,8 +214,8 @@ uint64_t llref_adjacency(void* gp, int dir, int level, uint64_t* off,
 
 void llref_degrees(void* gp, int level, uint32_t* deg) {
 	RefGraph* g = (RefGraph*)gp;
-	ll_mlcsr_ro_graph S(g->G, level);
-	for (uint64_t v = 0; v < g->V; v++) deg[v] = (uint32_t)S.out_degree(v);
+	View view(g, level);
+	for (uint64_t v = 0; v < g->V; v++) deg[v] = (uint32_t)view.g->out_degree(v);
 }
 
 void llref_set_threads(int n) { if (n > 0) omp_set_num_threads(n); }
@@ -204,9 +224,9 @@ int llref_max_threads(void) { return omp_get_max_threads(); }
 // "pagerank_double" (benchmark.cc:936-938): returns run() seconds.
 double llref_pagerank(void* gp, int level, int iters, double d, double* out) {
 	RefGraph* g = (RefGraph*)gp;
-	ll_mlcsr_ro_graph S(g->G, level);
+	View view(g, level);
 	ll_b_pagerank_pull_double<ll_mlcsr_ro_graph> b(iters, d);
-	b.initialize(&S);
+	b.initialize(view.g);
 	double t0 = now_s();
 	b.run();
 	double t = now_s() - t0;
@@ -218,7 +238,8 @@ double llref_pagerank(void* gp, int level, int iters, double d, double* out) {
 // "sssp_unweighted" levels via u_sssp_bfs (sssp.h:219-300): returns seconds.
 double llref_bfs_levels(void* gp, int level, int64_t root, int32_t* dist) {
 	RefGraph* g = (RefGraph*)gp;
-	ll_mlcsr_ro_graph S(g->G, level);
+	View view(g, level);
+	ll_mlcsr_ro_graph& S = *view.g;
 	for (uint64_t v = 0; v < g->V; v++) dist[v] = INT_MAX - 1;
 	node_t r = root;
 	dist[r] = 0;
@@ -232,9 +253,9 @@ double llref_bfs_levels(void* gp, int level, int64_t root, int32_t* dist) {
 // "bfs_count" (bfs.h:117-127): returns the count; *secs = run() seconds.
 double llref_bfs_count(void* gp, int level, int64_t root, double* secs) {
 	RefGraph* g = (RefGraph*)gp;
-	ll_mlcsr_ro_graph S(g->G, level);
+	View view(g, level);
 	ll_b_bfs<ll_mlcsr_ro_graph> b(root);
-	b.initialize(&S);
+	b.initialize(view.g);
 	double t0 = now_s();
 	double r = b.run();
 	if (secs) *secs = now_s() - t0;

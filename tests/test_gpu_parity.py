@@ -1,0 +1,158 @@
+"""GPU parity: the CUDA engine through the C ABI against the reference's
+golden outputs and the CPU oracle.
+
+Bars: adjacency, degrees and BFS levels bit-exact; FP64 PageRank within 1e-12
+max relative error (only the summation order differs from the reference).
+"""
+import numpy as np
+import pytest
+
+import llama_b200 as lb
+from llama_b200 import HostGraph, Store, workloads
+from oracle.bind import Oracle
+from tests._util import max_rel_err
+
+pytestmark = pytest.mark.gpu
+
+PR_TOL = 1e-12
+
+
+def device_store(levels, V):
+    hg = HostGraph(V)
+    for lv in levels:
+        hg.add_level(*lv)
+    st = Store()
+    st.ingest(hg)
+    return hg, st
+
+
+def test_golden_snapshots(golden):
+    V = int(golden["V"])
+    hg, st = device_store(golden["levels"], V)
+    with st:
+        for l in range(len(golden["levels"])):
+            with st.snapshot(l) as sn:
+                for dr in (0, 1):
+                    off, nb = sn.adjacency(dr)
+                    assert np.array_equal(off, golden[f"adj{l}_{dr}_off"]), (l, dr)
+                    assert np.array_equal(nb, golden[f"adj{l}_{dr}_nbr"]), (l, dr)
+                assert np.array_equal(sn.out_degrees(), golden[f"outdeg{l}"])
+                pr = sn.pagerank_pull(int(golden["pr_iters"]), float(golden["damping"]))
+                assert max_rel_err(pr, golden[f"pr{l}"]) <= PR_TOL, l
+                for i, r in enumerate(golden["roots"]):
+                    lv, res = sn.bfs(int(r))
+                    assert np.array_equal(lv, golden[f"bfs{l}"][i]), (l, r)
+                    assert res.reached == golden[f"bfscount{l}"][i]
+
+
+def _oracle_for(hg):
+    O = Oracle(hg.max_nodes)
+    for l in range(hg.num_levels):
+        O.add_level(*hg.level_input(l)[:4])
+    return O
+
+
+def test_rmat16_single_level_pagerank_bfs():
+    """R-MAT scale 16, one level: PageRank FP64 10 iterations, BFS from 0."""
+    spec = workloads.rmat_single_level(scale=16, seed=1)
+    hg = HostGraph.from_spec(spec)
+    O = _oracle_for(hg)
+    with Store() as st:
+        st.ingest(hg)
+        with st.snapshot() as sn:
+            assert sn.stats(1)["hubs"] > 0          # exercises the hub CTAs
+            pr = sn.pagerank_pull(10, 0.85)
+            assert max_rel_err(pr, O.pagerank_pull(0, 10, 0.85)) <= PR_TOL
+            lv, res = sn.bfs(0)
+            ref, reached = O.bfs(0, 0)
+            assert np.array_equal(lv, ref)
+            assert res.reached == reached
+
+
+def test_multiversion_with_deletions_every_snapshot():
+    spec = workloads.rmat_multiversion(scale=15, seed=2, levels=8, level0=0.9, delete=0.01)
+    hg = HostGraph.from_spec(spec)
+    O = _oracle_for(hg)
+    with Store() as st:
+        st.ingest(hg)
+        for l in (0, 3, 7):
+            with st.snapshot(l) as sn:
+                off, nb = sn.adjacency(0)
+                o_off, o_nb, _ = O.adjacency(l, 0)
+                assert np.array_equal(off, o_off) and np.array_equal(nb, o_nb)
+                off, nb = sn.adjacency(1)
+                o_off, o_nb, _ = O.adjacency(l, 1)
+                assert np.array_equal(off, o_off) and np.array_equal(nb, o_nb)
+                assert np.array_equal(sn.in_degrees(), O.degrees(l, 1))
+                pr = sn.pagerank_pull(20, 0.85)
+                assert max_rel_err(pr, O.pagerank_pull(l, 20, 0.85)) <= PR_TOL
+                deg = sn.out_degrees()
+                for r in workloads.pick_roots(deg, 4, seed=3):
+                    lv, res = sn.bfs(int(r))
+                    ref, reached = O.bfs(l, int(r))
+                    assert np.array_equal(lv, ref), (l, r)
+                    assert res.reached == reached
+
+
+def test_device_outputs_and_reuse():
+    """Outputs written straight into torch CUDA tensors; repeated calls agree."""
+    import torch
+    spec = workloads.rmat_multiversion(scale=14, seed=4, levels=3, level0=0.8, delete=0.02)
+    hg = HostGraph.from_spec(spec)
+    with Store() as st:
+        st.ingest(hg)
+        with st.snapshot() as sn:
+            host = sn.pagerank_pull(7)
+            dev = torch.empty(sn.max_nodes, dtype=torch.float64, device="cuda")
+            sn.pagerank_pull(7, out=dev)
+            st.sync()
+            assert np.array_equal(dev.cpu().numpy(), host)   # deterministic
+            lv_dev = torch.empty(sn.max_nodes, dtype=torch.int32, device="cuda")
+            _, r1 = sn.bfs(5, out=lv_dev)
+            st.sync()
+            lv, r2 = sn.bfs(5)
+            assert np.array_equal(lv_dev.cpu().numpy(), lv)
+            assert r1.reached == r2.reached
+
+
+def test_incremental_ingest_and_drop_level():
+    spec = workloads.rmat_multiversion(scale=13, seed=5, levels=4, level0=0.7, delete=0.05)
+    hg = HostGraph.from_spec(spec)
+    O = _oracle_for(hg)
+    with Store() as st:
+        for l in range(4):
+            st.ingest_level(hg.level_desc(l))
+            with st.snapshot() as sn:
+                assert sn.level == l
+                assert max_rel_err(sn.pagerank_pull(5), O.pagerank_pull(l, 5)) <= PR_TOL
+        st.drop_level()
+        st.drop_level()
+        assert st.num_levels == 2
+        with st.snapshot() as sn:
+            off, nb = sn.adjacency(0)
+            o_off, o_nb, _ = O.adjacency(1, 0)
+            assert np.array_equal(nb, o_nb)
+        st.ingest_level(hg.level_desc(2))
+        with st.snapshot() as sn:
+            assert max_rel_err(sn.pagerank_pull(5), O.pagerank_pull(2, 5)) <= PR_TOL
+
+
+def test_errors_are_reported_not_faulted():
+    spec = workloads.rmat_single_level(scale=10, seed=1)
+    hg = HostGraph.from_spec(spec)
+    with Store() as st:
+        st.ingest(hg)
+        with st.snapshot() as sn:
+            with pytest.raises(lb.LgError):
+                sn.bfs(1 << 10)
+            with pytest.raises(lb.LgError):
+                sn.pagerank_pull(3, damping=1.5)
+            with pytest.raises(lb.LgError):
+                st.drop_level()                   # snapshot still open
+        with pytest.raises(lb.LgError):
+            st.snapshot(3)
+        # a level whose vertex table points past its edge table is rejected
+        d = hg.level_desc(0)
+        d.out.n_slots = 1
+        with pytest.raises(lb.LgError):
+            st.ingest_level(d)
