@@ -45,6 +45,11 @@ def lgo():
             ("lgo_degrees", None, [_P, _INT, _INT, _P]),
             ("lgo_pagerank_pull", None, [_P, _INT, _INT, _D, _P]),
             ("lgo_bfs", _U64, [_P, _INT, _I64, _P]),
+            ("lgo_bc", None, [_P, _INT, _P, _INT, _P]),
+            ("lgo_sssp", _U64, [_P, _INT, _I64, _P]),
+            ("lgo_tc", _I64, [_P, _INT]),
+            ("lgo_scc", None, [_P, _INT, _P]),
+            ("lgo_ppr", None, [_P, _INT, _P, _INT, _INT, _D, _P]),
         ]:
             f = getattr(L, name)
             f.restype, f.argtypes = res, args
@@ -73,6 +78,11 @@ def ref():
             ("llref_pagerank", _D, [_P, _INT, _INT, _D, _P]),
             ("llref_bfs_levels", _D, [_P, _INT, _I64, _P]),
             ("llref_bfs_count", _D, [_P, _INT, _I64, C.POINTER(_D)]),
+            ("llref_add_level_weighted", _INT, [_P, _P, _P, _U64, _P, _P, _U64, _P]),
+            ("llref_sssp", _D, [_P, _INT, _I64, _P]),
+            ("llref_bc", _D, [_P, _INT, _P, _INT, _P]),
+            ("llref_tc_u", _I64, [_P, C.POINTER(_D)]),
+            ("llref_tarjan_scc", _D, [_P, _INT]),
         ]:
             f = getattr(L, name)
             f.restype, f.argtypes = res, args
@@ -148,6 +158,31 @@ class Oracle(_Base):
         reached = lgo().lgo_bfs(self.h, level, int(root), _p(out))
         return out, reached
 
+    def bc(self, level, sources):
+        src = np.ascontiguousarray(sources, np.int64)
+        out = np.empty(self.V, np.float64)
+        lgo().lgo_bc(self.h, level, _p(src), len(src), _p(out))
+        return out
+
+    def sssp(self, level, root):
+        out = np.empty(self.V, np.uint32)
+        reached = lgo().lgo_sssp(self.h, level, int(root), _p(out))
+        return out, reached
+
+    def tc(self, level):
+        return lgo().lgo_tc(self.h, level)
+
+    def scc(self, level):
+        out = np.empty(self.V, np.int64)
+        lgo().lgo_scc(self.h, level, _p(out))
+        return out
+
+    def ppr(self, level, seeds, iterations, damping=0.85):
+        s = np.ascontiguousarray(seeds, np.int64)
+        out = np.empty((self.V, len(s)), np.float64)
+        lgo().lgo_ppr(self.h, level, _p(s), len(s), iterations, damping, _p(out))
+        return out
+
 
 class Reference(_Base):
     """The reference's own code compiled from source (oracle/_ref)."""
@@ -177,9 +212,33 @@ class Reference(_Base):
         s, d, ds, dd = _u32(src), _u32(dst), _u32(del_src), _u32(del_dst)
         order = np.lexsort((d, s))
         s, d = np.ascontiguousarray(s[order]), np.ascontiguousarray(d[order])
-        r = ref().llref_add_level(self.h, _p(s), _p(d), len(s), _p(ds), _p(dd), len(ds))
+        if weights is None:
+            r = ref().llref_add_level(self.h, _p(s), _p(d), len(s), _p(ds), _p(dd), len(ds))
+        else:
+            w = np.ascontiguousarray(_u32(weights)[order])
+            r = ref().llref_add_level_weighted(self.h, _p(s), _p(d), len(s), _p(ds),
+                                               _p(dd), len(ds), _p(w))
         if r != 0:
             raise ValueError(f"reference harness rejected the level ({r})")
+
+    def sssp(self, level, root):
+        out = np.empty(self.V, np.uint32)
+        secs = ref().llref_sssp(self.h, level, int(root), _p(out))
+        return out, secs
+
+    def bc(self, level, sources):
+        src = np.ascontiguousarray(sources, np.int64)
+        out = np.empty(self.V, np.float32)
+        secs = ref().llref_bc(self.h, level, _p(src), len(src), _p(out))
+        return out, secs
+
+    def tc_u(self):
+        secs = _D()
+        n = ref().llref_tc_u(self.h, C.byref(secs))
+        return n, secs.value
+
+    def tarjan_scc_seconds(self, level=-1):
+        return ref().llref_tarjan_scc(self.h, level)
 
     def level_arrays(self, level, direction=0):
         n = ref().llref_level_arrays(self.h, direction, level, None, None)

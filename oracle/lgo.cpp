@@ -371,4 +371,208 @@ uint64_t lgo_bfs(void* gp, int level, int64_t root, int32_t* dist) {
 	return reached;
 }
 
+// Brandes betweenness centrality from explicit sources, FP64 restatement of
+// bc_random_bfs (bc_random.h:55-111) over ll_bfs_template's level-synchronous
+// BFS: sigma is pushed along down edges (level[w] == level[v] + 1, the edges
+// is_down_edge marks, ll_bfs_template.h:337-351); the reverse sweep visits
+// levels deepest first and sets delta[v] = sum over down edges v->w of
+// sigma[v] / sigma[w] * (1 + delta[w]), then BC[v] += delta[v] for v != s.
+void lgo_bc(void* gp, int level, const int64_t* sources, int n, double* bc) {
+	Graph* g = (Graph*)gp;
+	const uint64_t V = g->V;
+	std::vector<int32_t> lev(V);
+	std::vector<double> sigma(V), delta(V);
+	std::vector<uint32_t> nb;
+	for (uint64_t v = 0; v < V; v++) bc[v] = 0.0;
+	for (int i = 0; i < n; i++) {
+		const int64_t s = sources[i];
+		std::fill(lev.begin(), lev.end(), -1);
+		std::fill(sigma.begin(), sigma.end(), 0.0);
+		std::vector<std::vector<uint32_t>> levels(1, std::vector<uint32_t>(1, (uint32_t)s));
+		lev[s] = 0;
+		sigma[s] = 1.0;
+		for (int32_t cur = 0; !levels[cur].empty(); cur++) {
+			levels.emplace_back();
+			for (uint32_t v : levels[cur]) {
+				neighbours(g->out, level, v, nb, nullptr);
+				for (uint32_t w : nb)
+					if (lev[w] < 0) { lev[w] = cur + 1; levels[cur + 1].push_back(w); }
+			}
+			for (uint32_t v : levels[cur]) {          // visit_fw
+				neighbours(g->out, level, v, nb, nullptr);
+				for (uint32_t w : nb)
+					if (lev[w] == cur + 1) sigma[w] += sigma[v];
+			}
+		}
+		for (int32_t cur = (int32_t)levels.size() - 1; cur >= 0; cur--) {   // visit_rv
+			for (uint32_t v : levels[cur]) {
+				if ((int64_t)v == s) continue;
+				double S = 0.0;
+				neighbours(g->out, level, v, nb, nullptr);
+				for (uint32_t w : nb)
+					if (lev[w] == cur + 1) S = S + sigma[v] / sigma[w] * (1 + delta[w]);
+				delta[v] = S;
+				bc[v] = bc[v] + delta[v];
+			}
+		}
+	}
+}
+
+// Weighted SSSP: ll_b_sssp_weighted::run (sssp.h:97-183), frontier
+// Bellman-Ford to a fixpoint with G_len[e] = the per-slot edge property
+// (ll_mlcsr_properties.h:985-1005).  dist = INT_MAX-1 when unreached.
+// Returns the number of reached vertices (the finalize() value).
+uint64_t lgo_sssp(void* gp, int level, int64_t root, uint32_t* dist_out) {
+	Graph* g = (Graph*)gp;
+	const uint64_t V = g->V;
+	const uint64_t INF = UNREACHED;
+	std::vector<uint64_t> dist(V, INF), nxt(V, INF);
+	std::vector<char> upd(V, 0), upd_n(V, 0);
+	dist[root] = nxt[root] = 0;
+	upd[root] = 1;
+	std::vector<uint32_t> nb;
+	std::vector<int64_t> ids;
+	bool fin = false;
+	while (!fin) {
+		for (uint64_t n = 0; n < V; n++) {
+			if (!upd[n]) continue;
+			neighbours(g->out, level, n, nb, &ids);
+			for (size_t k = 0; k < nb.size(); k++) {
+				uint64_t w = g->out.w[edge_level(ids[k])][edge_index(ids[k])];
+				uint64_t cand = dist[n] + w;
+				if (nxt[nb[k]] > cand) { nxt[nb[k]] = cand; upd_n[nb[k]] = 1; }
+			}
+		}
+		bool any = false;
+		for (uint64_t t = 0; t < V; t++) {
+			dist[t] = nxt[t];
+			upd[t] = upd_n[t];
+			upd_n[t] = 0;
+			any = any || upd[t];
+		}
+		fin = !any;
+	}
+	uint64_t count = 0;
+	for (uint64_t v = 0; v < V; v++) {
+		dist_out[v] = (uint32_t)dist[v];
+		count += dist[v] < INF;
+	}
+	return count;
+}
+
+// Triangle counting on the symmetrised, de-duplicated snapshot (what tc_u
+// computes on a graph loaded with -U and flattened to one level,
+// triangle_counting.h:343-470): triangles u < v < w with all three
+// undirected edges present, each counted once.
+int64_t lgo_tc(void* gp, int level) {
+	Graph* g = (Graph*)gp;
+	const uint64_t V = g->V;
+	std::vector<std::vector<uint32_t>> adj(V);
+	std::vector<uint32_t> nb;
+	for (uint64_t v = 0; v < V; v++) {
+		neighbours(g->out, level, v, nb, nullptr);
+		for (uint32_t w : nb)
+			if (w != v) { adj[v].push_back(w); adj[w].push_back((uint32_t)v); }
+	}
+	for (auto& a : adj) {
+		std::sort(a.begin(), a.end());
+		a.erase(std::unique(a.begin(), a.end()), a.end());
+	}
+	int64_t T = 0;
+	for (uint64_t u = 0; u < V; u++)
+		for (uint32_t v : adj[u]) {
+			if (v <= u) continue;
+			// count_for: common neighbours of u and v greater than v
+			size_t i = 0, j = 0;
+			const auto &A = adj[u], &B = adj[v];
+			while (i < A.size() && j < B.size()) {
+				if (A[i] < B[j]) i++;
+				else if (B[j] < A[i]) j++;
+				else { if (A[i] > v) T++; i++; j++; }
+			}
+		}
+	return T;
+}
+
+// Strongly connected components of the snapshot, labelled by the smallest
+// vertex id of each component.  The reference's tarjan_scc
+// (tarjan_scc.h:55-206) uses vertex ids as low-links and does not compute
+// true SCCs, so this is a plain iterative Tarjan with discovery indices.
+void lgo_scc(void* gp, int level, int64_t* label) {
+	Graph* g = (Graph*)gp;
+	const uint64_t V = g->V;
+	std::vector<std::vector<uint32_t>> adj(V);
+	for (uint64_t v = 0; v < V; v++) neighbours(g->out, level, v, adj[v], nullptr);
+	std::vector<int64_t> idx(V, -1), low(V, 0);
+	std::vector<char> on(V, 0);
+	std::vector<uint32_t> stk;
+	std::vector<std::pair<uint32_t, size_t>> call;
+	int64_t counter = 0;
+	for (uint64_t r = 0; r < V; r++) {
+		if (idx[r] >= 0) continue;
+		call.push_back({(uint32_t)r, 0});
+		idx[r] = low[r] = counter++;
+		stk.push_back((uint32_t)r);
+		on[r] = 1;
+		while (!call.empty()) {
+			uint32_t v = call.back().first;
+			size_t& k = call.back().second;
+			if (k < adj[v].size()) {
+				uint32_t w = adj[v][k++];
+				if (idx[w] < 0) {
+					idx[w] = low[w] = counter++;
+					stk.push_back(w);
+					on[w] = 1;
+					call.push_back({w, 0});
+				} else if (on[w]) {
+					low[v] = std::min(low[v], idx[w]);
+				}
+			} else {
+				if (low[v] == idx[v]) {
+					std::vector<uint32_t> comp;
+					uint32_t w;
+					do { w = stk.back(); stk.pop_back(); on[w] = 0; comp.push_back(w); }
+					while (w != v);
+					int64_t m = *std::min_element(comp.begin(), comp.end());
+					for (uint32_t x : comp) label[x] = m;
+				}
+				call.pop_back();
+				if (!call.empty()) {
+					uint32_t p = call.back().first;
+					low[p] = std::min(low[p], low[v]);
+				}
+			}
+		}
+	}
+}
+
+// Personalized PageRank with K single-vertex teleport seeds, the pull
+// iteration of pagerank.h:120-169 with the uniform teleport (1-d)/N replaced
+// by (1-d) * [t == seed_k]: x0 = e_seed, then `iters` times
+// x'[t] = (1-d) [t == seed] + d * sum_{w in in(t)} x[w] / out_degree(w).
+// out is vertex-major: out[v * K + k].
+void lgo_ppr(void* gp, int level, const int64_t* seeds, int K, int iters,
+		double d, double* out) {
+	Graph* g = (Graph*)gp;
+	const uint64_t V = g->V;
+	std::vector<double> x(V), nx(V);
+	std::vector<uint32_t> nb;
+	std::vector<std::vector<uint32_t>> in(V);
+	for (uint64_t t = 0; t < V; t++) neighbours(g->in, level, t, in[t], nullptr);
+	for (int k = 0; k < K; k++) {
+		std::fill(x.begin(), x.end(), 0.0);
+		x[seeds[k]] = 1.0;
+		for (int it = 0; it < iters; it++) {
+			for (uint64_t t = 0; t < V; t++) {
+				double S = 0.0;
+				for (uint32_t w : in[t])
+					S = S + x[w] / ((double)g->out.vt[level][w].degree);
+				nx[t] = ((int64_t)t == seeds[k] ? (1 - d) : 0.0) + d * S;
+			}
+			x.swap(nx);
+		}
+		for (uint64_t v = 0; v < V; v++) out[v * K + k] = x[v];
+	}
+}
+
 } // extern "C"

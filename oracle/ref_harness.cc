@@ -28,6 +28,9 @@
 #include "benchmarks/bfs.h"
 #include "benchmarks/sssp.h"
 #include "benchmarks/pagerank.h"
+#include "benchmarks/bc_random.h"
+#include "benchmarks/triangle_counting.h"
+#include "benchmarks/tarjan_scc.h"
 
 // The per-vertex result arrays of the benchmark classes are private members.
 // An explicit template instantiation may name a private member (C++ [temp.
@@ -44,11 +47,19 @@ struct PrRankTag {
 template struct Reader<PrRankTag,
 	&ll_b_pagerank_pull_ext<ll_mlcsr_ro_graph, double>::G_pg_rank>;
 
+struct SsspDistTag {
+	typedef float* ll_b_sssp_weighted<ll_mlcsr_ro_graph, float>::*type;
+	friend type get(SsspDistTag);
+};
+template struct Reader<SsspDistTag,
+	&ll_b_sssp_weighted<ll_mlcsr_ro_graph, float>::G_dist>;
+
 namespace {
 
 struct RefGraph {
 	uint64_t V;
 	ll_mlcsr_ro_graph* G;
+	ll_mlcsr_edge_property<uint32_t>* weight;   // "weight", LL_T_FLOAT, or NULL
 };
 
 double now_s() {
@@ -94,7 +105,38 @@ void* llref_create(uint64_t V) {
 	RefGraph* g = new RefGraph();
 	g->V = V;
 	g->G = new ll_mlcsr_ro_graph((ll_database*)NULL);
+	g->weight = NULL;
 	return g;
+}
+
+// Append a level with a per-edge weight (uint32, stored as the float edge
+// property "weight" that sssp_weighted reads, benchmark.cc:1486-1488).  The
+// property level is initialised like a checkpoint does
+// (ll_mlcsr_graph.h:1583-1588) and written with cow_write by edge id.
+int llref_add_level(void* gp, const uint32_t* src, const uint32_t* dst,
+		uint64_t n, const uint32_t* dsrc, const uint32_t* ddst, uint64_t nd);
+int llref_add_level_weighted(void* gp, const uint32_t* src, const uint32_t* dst,
+		uint64_t n, const uint32_t* dsrc, const uint32_t* ddst, uint64_t nd,
+		const uint32_t* w) {
+	RefGraph* g = (RefGraph*)gp;
+	ll_mlcsr_ro_graph& G = *g->G;
+	const int level = (int)G.num_levels();
+	if (level == 0)
+		g->weight = G.create_uninitialized_edge_property_32("weight", LL_T_FLOAT);
+	if (g->weight == NULL) return -3;
+	int r = llref_add_level(gp, src, dst, n, dsrc, ddst, nd);
+	if (r) return r;
+	g->weight->cow_init_level(G.out().max_edges(level));
+	for (uint64_t i = 0; i < n; i++) {
+		edge_t e = G.out().find(src[i], dst[i]);
+		if (e == LL_NIL_EDGE || LL_EDGE_LEVEL(e) != (size_t)level) return -4;
+		float f = (float)w[i];
+		uint32_t bits;
+		memcpy(&bits, &f, 4);
+		g->weight->cow_write(e, bits);
+	}
+	g->weight->cow_finish_level();
+	return 0;
 }
 
 void llref_destroy(void* gp) {
@@ -260,6 +302,81 @@ double llref_bfs_count(void* gp, int level, int64_t root, double* secs) {
 	double r = b.run();
 	if (secs) *secs = now_s() - t0;
 	return r;
+}
+
+} // extern "C"
+
+extern "C" {
+
+// "sssp_weighted" (ll_b_sssp_weighted<Graph, float>, sssp.h:59-216) from
+// `root`; distances written as uint32 (exact: integer weights, sums < 2^24),
+// INT_MAX - 1 when unreached.  Returns run() seconds.
+double llref_sssp(void* gp, int level, int64_t root, uint32_t* dist) {
+	RefGraph* g = (RefGraph*)gp;
+	View view(g, level);
+	ll_b_sssp_weighted<ll_mlcsr_ro_graph, float> b(root, "weight");
+	b.initialize(view.g);
+	double t0 = now_s();
+	b.run();
+	double t = now_s() - t0;
+	float* d = b.*get(SsspDistTag());
+	for (uint64_t v = 0; v < g->V; v++)
+		dist[v] = d[v] < (float)(INT_MAX - 1) ? (uint32_t)d[v] : (uint32_t)(INT_MAX - 1);
+	return t;
+}
+
+// Brandes BC from explicit sources: the body of ll_b_bc_random::run
+// (bc_random.h:158-193) with the given sources in place of
+// pick_random_node().  FP32, as in the reference.  Returns seconds.
+double llref_bc(void* gp, int level, const int64_t* sources, int n, float* bc) {
+	RefGraph* g = (RefGraph*)gp;
+	View view(g, level);
+	ll_mlcsr_ro_graph& G = *view.g;
+	const uint64_t V = g->V;
+	float* G_BC = bc;
+	std::vector<float> sig(V), del(V);
+	float* G_sigma = sig.data();
+	float* G_delta = del.data();
+	double t0 = now_s();
+#pragma omp parallel for
+	for (node_t t = 0; t < (node_t)V; t++) G_BC[t] = 0;
+	for (int k = 0; k < n; k++) {
+		node_t s = sources[k];
+#pragma omp parallel for
+		for (node_t t = 0; t < (node_t)V; t++) G_sigma[t] = 0;
+		G_sigma[s] = 1;
+		bc_random_bfs<ll_mlcsr_ro_graph> bfs(G, G_BC, s, G_sigma, G_delta);
+		bfs.prepare(s);
+		bfs.do_bfs_forward();
+		bfs.do_bfs_reverse();
+	}
+	return now_s() - t0;
+}
+
+// "tc_u" (ll_b_triangle_counting_LU, triangle_counting.h:343-470); the store
+// must hold exactly one level with symmetric, sorted adjacency.  Returns the
+// triangle count; *secs = run() seconds.
+int64_t llref_tc_u(void* gp, double* secs) {
+	RefGraph* g = (RefGraph*)gp;
+	if (g->G->num_levels() != 1) return -1;
+	ll_b_triangle_counting_LU<ll_mlcsr_ro_graph> b;
+	b.initialize(g->G);
+	double t0 = now_s();
+	double r = b.run();
+	if (secs) *secs = now_s() - t0;
+	return (int64_t)r;
+}
+
+// "tarjan_scc" (ll_b_tarjan_scc, tarjan_scc.h:121-206), timing only: its
+// labels are not true SCCs.  Returns run() seconds.
+double llref_tarjan_scc(void* gp, int level) {
+	RefGraph* g = (RefGraph*)gp;
+	View view(g, level);
+	ll_b_tarjan_scc<ll_mlcsr_ro_graph> b;
+	b.initialize(view.g);
+	double t0 = now_s();
+	b.run();
+	return now_s() - t0;
 }
 
 } // extern "C"

@@ -20,8 +20,8 @@ def load_golden(path):
     z = np.load(path)
     g = {k: z[k] for k in z.files}
     L = int(g["num_levels"])
-    g["levels"] = [(g[f"in{l}_src"], g[f"in{l}_dst"], g[f"in{l}_dsrc"], g[f"in{l}_ddst"])
-                   for l in range(L)]
+    g["levels"] = [(g[f"in{l}_src"], g[f"in{l}_dst"], g[f"in{l}_dsrc"], g[f"in{l}_ddst"],
+                    g[f"in{l}_w"]) for l in range(L)]
     g["name"] = os.path.basename(path)[:-4]
     return g
 

@@ -48,3 +48,32 @@ def test_bfs_levels_exact(golden):
             lv, reached = O.bfs(l, r)
             assert np.array_equal(lv, golden[f"bfs{l}"][i]), (l, r)
             assert reached == golden[f"bfscount{l}"][i]
+
+
+def test_sssp_distances_exact(golden):
+    O = build(golden)
+    for l in range(len(golden["levels"])):
+        for i, r in enumerate(golden["roots"]):
+            d, _ = O.sssp(l, r)
+            assert np.array_equal(d, golden[f"sssp{l}"][i]), (l, r)
+
+
+def test_bc_matches_reference_fp32(golden):
+    """The reference accumulates BC in FP32; the oracle in FP64."""
+    O = build(golden)
+    for l in range(len(golden["levels"])):
+        bc = O.bc(l, golden["bc_sources"])
+        ref = golden[f"bc{l}"].astype(np.float64)
+        assert np.all(np.abs(bc - ref) <= 1e-5 * np.maximum(np.abs(bc), 1.0)), l
+
+
+def test_triangle_count_exact(golden):
+    O = build(golden)
+    for l in range(len(golden["levels"])):
+        assert O.tc(l) == golden[f"tc{l}"], l
+
+
+def test_scc_partition_exact(golden):
+    O = build(golden)
+    for l in range(len(golden["levels"])):
+        assert np.array_equal(O.scc(l), golden[f"scc{l}"]), l

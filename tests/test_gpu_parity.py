@@ -151,8 +151,12 @@ def test_errors_are_reported_not_faulted():
                 st.drop_level()                   # snapshot still open
         with pytest.raises(lb.LgError):
             st.snapshot(3)
-        # a level whose vertex table points past its edge table is rejected
-        d = hg.level_desc(0)
-        d.out.n_slots = 1
+    # a level whose vertex table points past its edge table is rejected
+    d = hg.level_desc(0)
+    d.out.n_slots = 1
+    with Store() as st2:
         with pytest.raises(lb.LgError):
-            st.ingest_level(d)
+            st2.ingest_level(d)
+        assert st2.num_levels == 0
+        st2.ingest(hg)                            # the store stays usable
+        assert st2.num_levels == 1
