@@ -199,7 +199,7 @@ typedef struct lg_snapshot_stats {
 	                           records included                           */
 	uint64_t fragment_slots;/* slots covered by the vertices' fragments   */
 	uint64_t fragments;     /* (vertex, level) fragments                  */
-	uint64_t hubs;          /* vertices reduced by whole CTAs             */
+	uint64_t ranges;        /* 2048-slot work ranges of the slot space    */
 	uint64_t deletions;     /* deletion marks visible in the snapshot     */
 } lg_snapshot_stats;
 lg_status lg_snapshot_get_stats(const lg_snapshot* snap, int dir,
@@ -253,6 +253,43 @@ typedef struct lg_bfs_result {
 
 lg_status lg_bfs(lg_snapshot* snap, int64_t root, int32_t* levels,
 		lg_bfs_result* result);
+
+/* Weighted single-source shortest paths: task "sssp_weighted",
+ * ll_b_sssp_weighted::run (benchmark/benchmarks/sssp.h:97-183), whose
+ * frontier Bellman-Ford reads G_len[e], the per-slot edge property
+ * (llama/include/llama/ll_mlcsr_properties.h:985-1005).  Here the weights are
+ * the uint32 per-slot property ingested with the out-CSR (lg_csr_level.weights)
+ * and the algorithm is delta-stepping with bucket width `delta`; distances are
+ * exact.  dist: uint32[max_nodes], LG_UNREACHED when unreached.  Weights and
+ * path lengths must stay below 2^31 - 2.  result (may be NULL): reached
+ * vertices (the reference's finalize() value), sum of their out-degrees,
+ * largest finite distance, buckets visited, relaxation rounds, relaxations. */
+typedef struct lg_sssp_result {
+	uint64_t reached;
+	uint64_t reach_edges;
+	uint32_t max_dist;
+	int32_t  buckets;
+	int32_t  rounds;
+	int32_t  reserved;
+	uint64_t relaxations;
+} lg_sssp_result;
+
+lg_status lg_sssp_delta(lg_snapshot* snap, int64_t root, uint32_t delta,
+		uint32_t* dist, lg_sssp_result* result);
+
+/* Triangle counting on the symmetrised, de-duplicated snapshot: task "tc_u",
+ * ll_b_triangle_counting_LU::run (benchmark/benchmarks/triangle_counting.h:
+ * 343-470), which needs the graph loaded with -U and flattened to a single
+ * sorted level (triangle_counting.h:422-425, benchmark/tools/flatten.h); the
+ * flattening happens on the device.  result: the triangle count (each
+ * triangle u < v < w once), undirected edges, live arcs read. */
+typedef struct lg_tc_result {
+	int64_t  triangles;
+	uint64_t undirected_edges;
+	uint64_t arcs;
+} lg_tc_result;
+
+lg_status lg_triangle_count(lg_snapshot* snap, lg_tc_result* result);
 
 /* ---------------------------------------------------------------------------
  * Errors.

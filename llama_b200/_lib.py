@@ -68,10 +68,22 @@ class lg_bfs_result(C.Structure):
                 ("bottom_up_steps", C.c_int32), ("reserved", C.c_int32)]
 
 
+class lg_sssp_result(C.Structure):
+    _fields_ = [("reached", C.c_uint64), ("reach_edges", C.c_uint64),
+                ("max_dist", C.c_uint32), ("buckets", C.c_int32),
+                ("rounds", C.c_int32), ("reserved", C.c_int32),
+                ("relaxations", C.c_uint64)]
+
+
+class lg_tc_result(C.Structure):
+    _fields_ = [("triangles", C.c_int64), ("undirected_edges", C.c_uint64),
+                ("arcs", C.c_uint64)]
+
+
 class lg_snapshot_stats(C.Structure):
     _fields_ = [("max_nodes", C.c_uint64), ("live_edges", C.c_uint64),
                 ("slots", C.c_uint64), ("fragment_slots", C.c_uint64),
-                ("fragments", C.c_uint64), ("hubs", C.c_uint64),
+                ("fragments", C.c_uint64), ("ranges", C.c_uint64),
                 ("deletions", C.c_uint64)]
 
 
@@ -116,6 +128,8 @@ SIGNATURES = [
     ("lg_snapshot_adjacency", _INT, [_P, _INT, _P, _P, _P]),
     ("lg_pagerank_pull", _INT, [_P, _INT, _D, _P]),
     ("lg_bfs", _INT, [_P, _I64, _P, C.POINTER(lg_bfs_result)]),
+    ("lg_sssp_delta", _INT, [_P, _I64, C.c_uint32, _P, C.POINTER(lg_sssp_result)]),
+    ("lg_triangle_count", _INT, [_P, C.POINTER(lg_tc_result)]),
     ("lg_last_error", C.c_size_t, [C.c_char_p, C.c_size_t]),
     ("lg_status_string", C.c_char_p, [_INT]),
     ("lg_version", C.c_char_p, []),

@@ -10,11 +10,13 @@
 // unvisited vertex look for a parent among its in-neighbours (in-CSR) in a
 // frontier bitmap that stays resident in L2.
 #include "lg_device.cuh"
+#include "lg_expand.cuh"
 
 namespace lg {
 
 constexpr int32_t kUnreached = LG_UNREACHED;
 constexpr int kBfsThreads = 256;
+constexpr uint32_t kBfsRange = 1024;
 
 __global__ void bfs_init(int32_t* level, uint64_t V, uint32_t root,
 		uint32_t* queue, const uint32_t* outdeg, unsigned long long* ctr) {
@@ -47,24 +49,64 @@ __device__ __forceinline__ void warp_add_u64(unsigned long long x,
 	if ((threadIdx.x & 31) == 0 && x) atomicAdd(dst, x);
 }
 
-// ctr[0] = next frontier size, ctr[1] = sum of out-degrees of the next frontier
+// Fragment slots of every frontier entry (to be scanned into range offsets).
+__global__ void bfs_frontier_slots(SnapCsr out, const uint32_t* queue, uint32_t qlen,
+		uint32_t* cnt) {
+	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= qlen) return;
+	uint32_t f0;
+	cnt[i] = vertex_slots(out, __ldg(queue + i), &f0);
+}
+
+// Top-down step over the frontier's slot space cut into kBfsRange-slot
+// ranges, one warp each (lg_expand.cuh).  ctr[0] = next frontier size,
+// ctr[1] = sum of out-degrees of the next frontier.
 __global__ void __launch_bounds__(kBfsThreads)
-bfs_top_down(SnapCsr out, const uint32_t* queue, uint32_t qlen,
-		int32_t* level, uint32_t* next, unsigned long long* ctr, int32_t cur) {
+bfs_top_down(SnapCsr out, const uint32_t* queue, const uint32_t* fpos, uint32_t qlen,
+		uint32_t total, uint32_t nranges, int32_t* level, uint32_t* next,
+		unsigned long long* ctr, int32_t cur) {
 	const uint32_t lane = threadIdx.x & 31u;
-	const uint64_t i = ((uint64_t)blockIdx.x * (kBfsThreads / 32) + (threadIdx.x >> 5)) * 32 + lane;
-	const bool valid = i < qlen;
-	uint32_t cnt = 0, f0 = 0;
-	if (valid) cnt = vertex_slots(out, __ldg(queue + i), &f0);
+	const uint64_t r64 = (uint64_t)blockIdx.x * (kBfsThreads / 32) + (threadIdx.x >> 5);
+	if (r64 >= nranges) return;
+	const uint32_t r = (uint32_t)r64;
+	const bool last_range = r == nranges - 1;
+	const uint32_t ra = r * kBfsRange;
+	const uint32_t rb = last_range ? total : min(total, ra + kBfsRange);
+	uint32_t e_begin, e_end;
+	range_entries(fpos, qlen, ra, rb, last_range, &e_begin, &e_end);
+	const LevelTab* lt = out.lt;
 	unsigned long long mf = 0;
-	warp_expand(out, cnt, f0,
-		[&](bool act, uint32_t, uint32_t nbr, uint32_t, uint32_t) {
-			bool won = false;
-			if (act && __ldcg(level + nbr) == kUnreached)
-				won = atomicCAS(level + nbr, kUnreached, cur + 1) == kUnreached;
-			warp_append(won, nbr, next, ctr);
-			if (won) mf += __ldg(out.deg + nbr);
-		});
+	for (uint32_t ew = e_begin; ew < e_end; ew += 32) {
+		const Window w = load_window(out, queue, fpos, ew, e_end, ra, rb);
+		for (uint32_t base = w.lo; base < w.hi; base += 32 * kUnroll) {
+			uint32_t nb[kUnroll];
+			bool act[kUnroll];
+#pragma unroll
+			for (int u = 0; u < kUnroll; u++) {
+				const uint32_t k = base + u * 32 + lane;
+				uint32_t own, lv, idx;
+				locate_slot(out, w, k, &own, &lv, &idx);
+				act[u] = k < w.hi;
+				nb[u] = 0;
+				if (act[u]) {
+					const uint32_t word = __ldg(lt->del[lv] + (idx >> 5));
+					nb[u] = __ldg(lt->ids[lv] + idx);
+					act[u] = !((word >> (idx & 31)) & 1u);
+				}
+			}
+			int32_t seen[kUnroll];
+#pragma unroll
+			for (int u = 0; u < kUnroll; u++) seen[u] = act[u] ? __ldcg(level + nb[u]) : 0;
+#pragma unroll
+			for (int u = 0; u < kUnroll; u++) {
+				bool won = false;
+				if (act[u] && seen[u] == kUnreached)
+					won = atomicCAS(level + nb[u], kUnreached, cur + 1) == kUnreached;
+				warp_append(won, nb[u], next, ctr);
+				if (won) mf += __ldg(out.deg + nb[u]);
+			}
+		}
+	}
 	warp_add_u64(mf, ctr + 1);
 }
 
@@ -119,6 +161,10 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 	LG_TRY(sc[1].reserve(V * 4));
 	LG_TRY(sc[2].reserve(((V + 31) / 32) * 4));
 	LG_TRY(sc[3].reserve(4 * sizeof(unsigned long long)));
+	LG_TRY(sc[5].reserve(V * 4));
+	LG_TRY(sc[6].reserve((V + 1) * 4));
+	uint32_t* fcnt = sc[5].as<uint32_t>();
+	uint32_t* fpos = sc[6].as<uint32_t>();
 	const bool dev_out = is_device_pointer(levels);
 	int32_t* lvl = levels;
 	if (!dev_out) {
@@ -153,11 +199,19 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 			top_down = true;
 		LG_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st), "memset");
 		if (top_down) {
-			uint64_t warps = (qlen + 31) / 32;
-			bfs_top_down<<<grid_for(warps, kBfsThreads / 32), kBfsThreads, 0, st>>>(
-					out, q, (uint32_t)qlen, lvl, nq, ctr, cur);
+			// frontier slot offsets, then one warp per kBfsRange slots
+			bfs_frontier_slots<<<grid_for(qlen, 256), 256, 0, st>>>(out, q,
+					(uint32_t)qlen, fcnt);
+			uint64_t total = 0;
+			LG_TRY(exclusive_scan_u32(fcnt, fpos, qlen, sc[7], st, &total));
+			s->d2h_bytes += 8;
+			const uint32_t nranges = (uint32_t)((total + kBfsRange - 1) / kBfsRange);
+			if (nranges > 0)
+				bfs_top_down<<<grid_for(nranges, kBfsThreads / 32), kBfsThreads, 0, st>>>(
+						out, q, fpos, (uint32_t)qlen, (uint32_t)total, nranges, lvl, nq,
+						ctr, cur);
 			td_steps++;
-			s->launches++;
+			s->launches += 5;
 		} else {
 			LG_CUDA(cudaMemsetAsync(bits, 0, ((V + 31) / 32) * 4, st), "memset");
 			bfs_set_bits<<<grid_for(qlen, 256), 256, 0, st>>>(q, (uint32_t)qlen, bits);

@@ -16,6 +16,8 @@
 //                              continuation chain resolved newest-first
 //   del[l]     bitset over level l's slots, bit = max_visible_level <= L
 //   deg        V x u32         live degree (the vertex-table degree field)
+//   slot_off   (V + 1) x u32   prefix of per-vertex fragment lengths: the
+//                              virtual slot space balanced kernels cut up
 #ifndef LG_DEVICE_CUH_
 #define LG_DEVICE_CUH_
 
@@ -31,9 +33,6 @@ namespace lg {
 constexpr uint32_t kNoId = 0xffffffffu;
 constexpr int kLevelBits = 6;                 // level field of a fragment
 constexpr uint32_t kLevelMask = (1u << kLevelBits) - 1u;
-constexpr uint32_t kHubSlots = 4096;          // vertices with more slots are
-                                              // reduced by whole CTAs
-constexpr uint32_t kHubChunk = 4096;          // slots per hub CTA
 
 // Per-snapshot, per-direction table of level base pointers.
 struct LevelTab {
@@ -168,14 +167,12 @@ struct DevCsr {
 };
 
 struct SnapDir {
-	DevBuf frag_off, frags, deg, delbits, lt, hubs, hub_chunk_off;
+	DevBuf frag_off, frags, deg, delbits, lt, slot_off;
 	uint64_t n_frags = 0;
 	uint64_t n_edges = 0;          // live edges (sum of degrees)
 	uint64_t n_slots = 0;          // slots of levels 0..L
 	uint64_t n_frag_slots = 0;     // slots covered by fragments
 	uint64_t n_dels = 0;           // deletion marks visible at L
-	uint32_t n_hubs = 0;
-	uint32_t n_hub_chunks = 0;
 	bool present = false;
 	SnapCsr view() const {
 		SnapCsr s;

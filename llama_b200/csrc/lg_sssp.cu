@@ -1,0 +1,237 @@
+// lg_sssp.cu - single-source shortest paths with integer edge weights.
+//
+// Reference: ll_b_sssp_weighted::run (benchmark/benchmarks/sssp.h:97-183), a
+// frontier Bellman-Ford to a fixpoint with G_len[e] the per-slot edge
+// property (llama/include/llama/ll_mlcsr_properties.h:985-1005); dist[root] =
+// 0, unreached vertices keep INT_MAX - 1.  Shortest-path distances are
+// unique, so any correct algorithm yields the same array: this one is
+// delta-stepping (Meyer & Sanders) in the near/far-queue form.  Vertices
+// whose tentative distance is below the current bucket bound are relaxed
+// repeatedly from a near queue; improvements beyond the bound go to a far
+// pile that is split when the near queue drains, the bound then moving to
+// the bucket of the smallest distance left in the pile.  Relaxation is
+// atomicMin on 32-bit distances, so the result does not depend on thread
+// order.  Per-vertex stamps keep every vertex at most once in the near queue
+// of a round and at most once in the far pile, which bounds both by V.
+#include "lg_device.cuh"
+
+namespace lg {
+
+constexpr uint32_t kInf = LG_UNREACHED;
+constexpr int kSsspThreads = 256;
+
+__global__ void sssp_init(uint32_t* dist, uint32_t* stamp, uint32_t* fstamp,
+		uint64_t V, uint32_t root, uint32_t* queue) {
+	uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (v < V) {
+		dist[v] = (v == root) ? 0u : kInf;
+		stamp[v] = 0xffffffffu;
+		fstamp[v] = 0xffffffffu;
+	}
+	if (v == 0) queue[0] = root;
+}
+
+__device__ __forceinline__ void warp_push(bool take, uint32_t item,
+		uint32_t* queue, unsigned long long* len) {
+	unsigned m = __ballot_sync(0xffffffffu, take);
+	if (!m) return;
+	const uint32_t lane = threadIdx.x & 31u;
+	const int leader = __ffs(m) - 1;
+	unsigned long long base = 0;
+	if ((int)lane == leader) base = atomicAdd(len, (unsigned long long)__popc(m));
+	base = __shfl_sync(0xffffffffu, base, leader);
+	if (take) queue[base + __popc(m & ((1u << lane) - 1u))] = item;
+}
+
+// ctr[0] near-next length, ctr[1] far length (starts at the current pile
+// size), ctr[2] relaxations
+__global__ void __launch_bounds__(kSsspThreads)
+sssp_relax(SnapCsr out, const uint32_t* queue, uint32_t qlen, uint32_t* dist,
+		uint32_t* stamp, uint32_t* fstamp, uint32_t round, uint32_t epoch,
+		uint32_t hi, uint32_t* near_next, uint32_t* far, unsigned long long* ctr) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint64_t i = ((uint64_t)blockIdx.x * (kSsspThreads / 32) + (threadIdx.x >> 5)) * 32 + lane;
+	const bool valid = i < qlen;
+	uint32_t cnt = 0, f0 = 0, du = 0;
+	if (valid) {
+		const uint32_t u = __ldg(queue + i);
+		du = __ldcg(dist + u);
+		cnt = vertex_slots(out, u, &f0);
+	}
+	unsigned long long relax = 0;
+	warp_expand(out, cnt, f0,
+		[&](bool act, uint32_t o, uint32_t nbr, uint32_t lv, uint32_t idx) {
+			const uint32_t dsrc = __shfl_sync(0xffffffffu, du, o);
+			bool to_near = false, to_far = false;
+			if (act) {
+				const uint32_t nd = dsrc + __ldg(out.lt->w[lv] + idx);
+				if (nd < __ldcg(dist + nbr)) {
+					const uint32_t old = atomicMin(dist + nbr, nd);
+					relax++;
+					if (nd < old) {
+						if (nd < hi) to_near = atomicExch(stamp + nbr, round) != round;
+						else to_far = atomicExch(fstamp + nbr, epoch) != epoch;
+					}
+				}
+			}
+			warp_push(to_near, nbr, near_next, ctr);
+			warp_push(to_far, nbr, far, ctr + 1);
+		});
+	for (int o = 16; o > 0; o >>= 1) relax += __shfl_down_sync(0xffffffffu, relax, o);
+	if (lane == 0 && relax) atomicAdd(ctr + 2, relax);
+}
+
+// Split the far pile at bound `hi`: entries with lo <= dist < hi go to the
+// near queue (entries below lo were settled from a near queue after they
+// entered the pile), entries >= hi are kept, stamped with the new epoch, and
+// the smallest kept distance is reported in ctr[2].
+__global__ void sssp_split_far(const uint32_t* far, unsigned long long n,
+		const uint32_t* dist, uint32_t* stamp, uint32_t* fstamp, uint32_t round,
+		uint32_t epoch, uint32_t lo, uint32_t hi, uint32_t* near, uint32_t* keep,
+		unsigned long long* ctr) {
+	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	uint32_t v = 0, d = kInf;
+	if (i < n) { v = far[i]; d = __ldcg(dist + v); }
+	const bool near_take = i < n && d >= lo && d < hi
+		&& atomicExch(stamp + v, round) != round;
+	const bool keep_take = i < n && d >= hi && d < kInf
+		&& atomicExch(fstamp + v, epoch) != epoch;
+	warp_push(near_take, v, near, ctr);
+	warp_push(keep_take, v, keep, ctr + 1);
+	unsigned long long m = keep_take ? d : ~0ull;
+	for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_down_sync(0xffffffffu, m, o));
+	if ((threadIdx.x & 31) == 0 && m != ~0ull) atomicMin(ctr + 2, m);
+}
+
+__global__ void sssp_reach(const uint32_t* dist, const uint32_t* outdeg, uint64_t V,
+		unsigned long long* ctr) {
+	unsigned long long c = 0, e = 0, mx = 0;
+	for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V;
+			v += (uint64_t)gridDim.x * blockDim.x) {
+		uint32_t d = dist[v];
+		if (d < kInf) { c++; e += outdeg[v]; if (d > mx) mx = d; }
+	}
+	for (int o = 16; o > 0; o >>= 1) {
+		c += __shfl_down_sync(0xffffffffu, c, o);
+		e += __shfl_down_sync(0xffffffffu, e, o);
+		mx = max(mx, __shfl_down_sync(0xffffffffu, mx, o));
+	}
+	if ((threadIdx.x & 31) == 0) {
+		atomicAdd(ctr, c);
+		atomicAdd(ctr + 1, e);
+		atomicMax(ctr + 2, mx);
+	}
+}
+
+} // namespace lg
+
+using namespace lg;
+
+extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta,
+		uint32_t* dist, lg_sssp_result* result) {
+	clear_error();
+	if (!sn || !dist) return set_error(LG_EINVAL, "null argument");
+	if (root < 0 || (uint64_t)root >= sn->V)
+		return set_error(LG_EINVAL, "root %lld out of range", (long long)root);
+	if (delta == 0) return set_error(LG_EINVAL, "delta must be positive");
+	lg_store* s = sn->store;
+	for (int l = 0; l <= sn->level; l++)
+		if (!s->out.levels[l]->w.p)
+			return set_error(LG_ESTATE, "level %d of the out-CSR carries no edge weights", l);
+	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+	cudaStream_t st = s->stream;
+	const uint64_t V = sn->V;
+	DevBuf* sc = s->scratch;
+	LG_TRY(sc[0].reserve(V * 4));          // near queue
+	LG_TRY(sc[1].reserve(V * 4));          // next near queue
+	LG_TRY(sc[2].reserve(V * 4));          // far pile
+	LG_TRY(sc[3].reserve(V * 4));          // far pile being compacted
+	LG_TRY(sc[5].reserve(2 * V * 4));      // near and far stamps
+	LG_TRY(sc[6].reserve(8 * sizeof(unsigned long long)));
+	const bool dev_out = is_device_pointer(dist);
+	uint32_t* d = dist;
+	if (!dev_out) { LG_TRY(sc[4].reserve(V * 4)); d = sc[4].as<uint32_t>(); }
+	uint32_t* q = sc[0].as<uint32_t>();
+	uint32_t* qn = sc[1].as<uint32_t>();
+	uint32_t* far = sc[2].as<uint32_t>();
+	uint32_t* far2 = sc[3].as<uint32_t>();
+	uint32_t* stamp = sc[5].as<uint32_t>();
+	uint32_t* fstamp = stamp + V;
+	unsigned long long* ctr = sc[6].as<unsigned long long>();
+	const SnapCsr out = sn->view(0);
+
+	sssp_init<<<grid_for(V, 256), 256, 0, st>>>(d, stamp, fstamp, V, (uint32_t)root, q);
+	LG_CUDA(cudaGetLastError(), "sssp_init");
+	s->launches++;
+	uint64_t qlen = 1, flen = 0, relaxations = 0;
+	uint32_t hi = delta, round = 0, epoch = 0;
+	int buckets = 1;
+	unsigned long long h[3];
+	while (qlen > 0 || flen > 0) {
+		if (qlen == 0) {
+			// near queue drained: split the far pile at the next bound; if
+			// nothing falls below it, jump to the bucket of the smallest
+			// remaining distance and split again
+			uint32_t lo = hi;
+			hi = (hi > kInf - delta) ? kInf : hi + delta;
+			for (int attempt = 0; attempt < 2; attempt++) {
+				round++;
+				epoch++;
+				unsigned long long init[3] = {0, 0, ~0ull};
+				LG_CUDA(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st), "h2d");
+				s->h2d_bytes += sizeof(init);
+				sssp_split_far<<<grid_for(flen, 256), 256, 0, st>>>(far, flen, d, stamp,
+						fstamp, round, epoch, lo, hi, q, far2, ctr);
+				LG_CUDA(cudaGetLastError(), "sssp_split_far");
+				s->launches++;
+				LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+				LG_CUDA(cudaStreamSynchronize(st), "sssp split");
+				s->d2h_bytes += sizeof(h);
+				if (h[0] > V || h[1] > V) return set_error(LG_ECUDA, "sssp queue overflow");
+				qlen = h[0];
+				flen = h[1];
+				std::swap(far, far2);
+				buckets++;
+				if (qlen > 0 || flen == 0) break;
+				uint32_t mind = (uint32_t)h[2];
+				lo = (mind / delta) * delta;
+				hi = (lo > kInf - delta) ? kInf : lo + delta;
+			}
+			continue;
+		}
+		round++;
+		unsigned long long init[3] = {0, flen, 0};
+		LG_CUDA(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st), "h2d");
+		s->h2d_bytes += sizeof(init);
+		uint64_t warps = (qlen + 31) / 32;
+		sssp_relax<<<grid_for(warps, kSsspThreads / 32), kSsspThreads, 0, st>>>(
+				out, q, (uint32_t)qlen, d, stamp, fstamp, round, epoch, hi, qn, far, ctr);
+		LG_CUDA(cudaGetLastError(), "sssp_relax");
+		s->launches++;
+		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+		LG_CUDA(cudaStreamSynchronize(st), "sssp relax");
+		s->d2h_bytes += sizeof(h);
+		if (h[0] > V || h[1] > V) return set_error(LG_ECUDA, "sssp queue overflow");
+		qlen = h[0];
+		flen = h[1];
+		relaxations += h[2];
+		std::swap(q, qn);
+	}
+	LG_CUDA(cudaMemsetAsync(ctr, 0, 3 * sizeof(unsigned long long), st), "memset");
+	sssp_reach<<<592, 256, 0, st>>>(d, sn->out.deg.as<uint32_t>(), V, ctr);
+	LG_CUDA(cudaGetLastError(), "sssp_reach");
+	s->launches++;
+	LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+	s->d2h_bytes += sizeof(h);
+	if (!dev_out) LG_TRY(copy_out(s, dist, d, V * 4));
+	LG_CUDA(cudaStreamSynchronize(st), "sssp");
+	if (result) {
+		result->reached = h[0];
+		result->reach_edges = h[1];
+		result->max_dist = (uint32_t)h[2];
+		result->buckets = buckets;
+		result->rounds = (int32_t)round;
+		result->relaxations = relaxations;
+	}
+	return LG_OK;
+}

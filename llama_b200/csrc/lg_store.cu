@@ -393,20 +393,6 @@ __global__ void mark_deletions(const uint2* dels, uint64_t n, int L,
 	atomicOr(del_words[lv] + (d.x >> 5), 1u << (d.x & 31));
 }
 
-__global__ void find_hubs(const uint32_t* slots, uint64_t V, uint32_t thr,
-		uint32_t* hubs, uint32_t* n_hubs, uint32_t cap) {
-	uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	if (v >= V || slots[v] < thr) return;
-	uint32_t i = atomicAdd(n_hubs, 1u);
-	if (i < cap) hubs[i] = (uint32_t)v;
-}
-
-__global__ void gather_u32(const uint32_t* src, const uint32_t* idx, uint64_t n,
-		uint32_t* out) {
-	uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < n) out[i] = src[idx[i]];
-}
-
 __global__ void sum_u32(const uint32_t* x, uint64_t n, unsigned long long* out) {
 	unsigned long long s = 0;
 	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -477,26 +463,23 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 		LG_CUDA(cudaStreamSynchronize(st), "snapshot deletions");
 	}
 
-	// hub vertices (reduced by whole CTAs) and live edge count
-	DevBuf hub_tmp, counters;
-	LG_TRY(counters.reserve(4 * sizeof(unsigned long long)));
-	LG_CUDA(cudaMemsetAsync(counters.p, 0, 4 * sizeof(unsigned long long), st), "memset");
-	uint32_t cap = 1u << 20;
-	LG_TRY(hub_tmp.reserve(cap * sizeof(uint32_t)));
-	find_hubs<<<grid_for(V, B), B, 0, st>>>(slots.as<uint32_t>(), V, kHubSlots,
-			hub_tmp.as<uint32_t>(), (uint32_t*)counters.p, cap);
-	sum_u32<<<592, B, 0, st>>>(d.deg.as<uint32_t>(), V,
-			counters.as<unsigned long long>() + 1);
-	sum_u32<<<592, B, 0, st>>>(slots.as<uint32_t>(), V,
-			counters.as<unsigned long long>() + 2);
-	LG_CUDA(cudaGetLastError(), "hub scan");
-	s->launches += 3;
-	unsigned long long hc[3];
-	LG_CUDA(cudaMemcpyAsync(hc, counters.p, sizeof(hc), cudaMemcpyDeviceToHost, st), "d2h");
-	LG_CUDA(cudaStreamSynchronize(st), "hub scan");
-	uint32_t nh = (uint32_t)(hc[0] & 0xffffffffu);
-	d.n_edges = hc[1];
-	d.n_frag_slots = hc[2];
+	// per-vertex slot prefix (the virtual slot space the balanced kernels cut
+	// into ranges) and the live edge count
+	uint64_t total_slots = 0;
+	LG_TRY(d.slot_off.reserve((V + 1) * sizeof(uint32_t)));
+	LG_TRY(exclusive_scan_u32(slots.as<uint32_t>(), d.slot_off.as<uint32_t>(), V,
+			scan_tmp, st, &total_slots));
+	DevBuf counters;
+	LG_TRY(counters.reserve(sizeof(unsigned long long)));
+	LG_CUDA(cudaMemsetAsync(counters.p, 0, sizeof(unsigned long long), st), "memset");
+	sum_u32<<<592, B, 0, st>>>(d.deg.as<uint32_t>(), V, counters.as<unsigned long long>());
+	LG_CUDA(cudaGetLastError(), "degree sum");
+	s->launches += 4;
+	unsigned long long ne = 0;
+	LG_CUDA(cudaMemcpyAsync(&ne, counters.p, sizeof(ne), cudaMemcpyDeviceToHost, st), "d2h");
+	LG_CUDA(cudaStreamSynchronize(st), "snapshot sizes");
+	d.n_edges = ne;
+	d.n_frag_slots = total_slots;
 	d.n_slots = 0;
 	for (int l = 0; l <= L; l++) d.n_slots += csr.levels[l]->n_slots;
 	d.n_dels = 0;
@@ -504,30 +487,6 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 		uint32_t lv = x.y >> LG_BITS_LEVEL, ml = x.y & ((1u << LG_BITS_LEVEL) - 1u);
 		d.n_dels += ((int)lv <= L && (int)ml <= L);
 	}
-	if (nh > cap) return set_error(LG_ENOTSUP, "too many hub vertices");
-	std::vector<uint32_t> hubs(nh), hub_slots(nh);
-	LG_TRY(d.hubs.reserve(std::max<uint32_t>(nh, 1) * 4));
-	if (nh) {
-		// sorted hub list (deterministic order), then their slot counts
-		LG_CUDA(cudaMemcpy(hubs.data(), hub_tmp.p, nh * 4, cudaMemcpyDeviceToHost), "d2h");
-		std::sort(hubs.begin(), hubs.end());
-		LG_CUDA(cudaMemcpy(d.hubs.p, hubs.data(), nh * 4, cudaMemcpyHostToDevice), "h2d");
-		gather_u32<<<grid_for(nh, B), B, 0, st>>>(slots.as<uint32_t>(),
-				d.hubs.as<uint32_t>(), nh, hub_tmp.as<uint32_t>());
-		LG_CUDA(cudaGetLastError(), "gather hub slots");
-		s->launches++;
-		LG_CUDA(cudaMemcpyAsync(hub_slots.data(), hub_tmp.p, nh * 4,
-				cudaMemcpyDeviceToHost, st), "d2h");
-		LG_CUDA(cudaStreamSynchronize(st), "hub slots");
-	}
-	std::vector<uint32_t> chunk_off(nh + 1, 0);
-	for (uint32_t i = 0; i < nh; i++)
-		chunk_off[i + 1] = chunk_off[i] + (hub_slots[i] + kHubChunk - 1) / kHubChunk;
-	d.n_hubs = nh;
-	d.n_hub_chunks = chunk_off[nh];
-	LG_TRY(d.hub_chunk_off.reserve((nh + 1) * 4));
-	LG_CUDA(cudaMemcpy(d.hub_chunk_off.p, chunk_off.data(), (nh + 1) * 4,
-			cudaMemcpyHostToDevice), "h2d");
 	d.present = true;
 	return LG_OK;
 }
@@ -768,7 +727,7 @@ lg_status lg_snapshot_get_stats(const lg_snapshot* sn, int dir, lg_snapshot_stat
 	st->slots = d.n_slots;
 	st->fragment_slots = d.n_frag_slots;
 	st->fragments = d.n_frags;
-	st->hubs = d.n_hubs;
+	st->ranges = (d.n_frag_slots + 2047) / 2048;
 	st->deletions = d.n_dels;
 	return LG_OK;
 }

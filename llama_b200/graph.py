@@ -264,3 +264,16 @@ class Snapshot:
         r = _lib.lg_bfs_result()
         check(lib.lg_bfs(self._h, int(root), ptr(res), C.byref(r)))
         return res, r
+
+    def triangle_count(self):
+        """Task ``tc_u`` on the symmetrised snapshot; returns lg_tc_result."""
+        r = _lib.lg_tc_result()
+        check(lib.lg_triangle_count(self._h, C.byref(r)))
+        return r
+
+    def sssp(self, root, delta=32, out=None):
+        """Task ``sssp_weighted`` (delta-stepping); returns (dist, lg_sssp_result)."""
+        res = np.empty(self.max_nodes, np.uint32) if out is None else out
+        r = _lib.lg_sssp_result()
+        check(lib.lg_sssp_delta(self._h, int(root), int(delta), ptr(res), C.byref(r)))
+        return res, r

@@ -60,7 +60,8 @@ def test_rmat16_single_level_pagerank_bfs():
     with Store() as st:
         st.ingest(hg)
         with st.snapshot() as sn:
-            assert sn.stats(1)["hubs"] > 0          # exercises the hub CTAs
+            st1 = sn.stats(1)
+            assert st1["ranges"] > 1 and np.max(sn.in_degrees()) > 2048  # straddling vertices
             pr = sn.pagerank_pull(10, 0.85)
             assert max_rel_err(pr, O.pagerank_pull(0, 10, 0.85)) <= PR_TOL
             lv, res = sn.bfs(0)
@@ -160,3 +161,64 @@ def test_errors_are_reported_not_faulted():
         assert st2.num_levels == 0
         st2.ingest(hg)                            # the store stays usable
         assert st2.num_levels == 1
+
+
+def test_golden_sssp(golden):
+    V = int(golden["V"])
+    hg, st = device_store(golden["levels"], V)
+    with st:
+        for l in range(len(golden["levels"])):
+            with st.snapshot(l) as sn:
+                for i, r in enumerate(golden["roots"]):
+                    for delta in (1, 32, 1 << 20):
+                        d, res = sn.sssp(int(r), delta)
+                        assert np.array_equal(d, golden[f"sssp{l}"][i]), (l, r, delta)
+                    assert res.reached == int(np.sum(d < lb._lib.LG_UNREACHED))
+
+
+def test_sssp_multiversion_weights_vs_oracle():
+    spec = workloads.rmat_multiversion(scale=15, seed=7, levels=4, level0=0.85, delete=0.01,
+                                       weight_max=255)
+    hg = HostGraph.from_spec(spec)
+    O = Oracle(hg.max_nodes)
+    for l in range(hg.num_levels):
+        O.add_level(*hg.level_input(l))
+    with Store() as st:
+        st.ingest(hg)
+        with st.snapshot() as sn:
+            for r in workloads.pick_roots(sn.out_degrees(), 3, seed=8):
+                d, res = sn.sssp(int(r), 32)
+                ref, reached = O.sssp(3, int(r))
+                assert np.array_equal(d, ref)
+                assert res.reached == reached
+
+
+def test_sssp_needs_weights():
+    hg = HostGraph.from_spec(workloads.rmat_single_level(scale=8, seed=1))
+    with Store() as st:
+        st.ingest(hg)
+        with st.snapshot() as sn:
+            with pytest.raises(lb.LgError):
+                sn.sssp(0)
+
+
+def test_golden_triangles(golden):
+    V = int(golden["V"])
+    hg, st = device_store(golden["levels"], V)
+    with st:
+        for l in range(len(golden["levels"])):
+            with st.snapshot(l) as sn:
+                assert sn.triangle_count().triangles == golden[f"tc{l}"], l
+
+
+def test_triangles_multiversion_vs_oracle():
+    spec = workloads.rmat_multiversion(scale=14, seed=2, levels=8, level0=0.9, delete=0.01)
+    hg = HostGraph.from_spec(spec)
+    O = _oracle_for(hg)
+    with Store() as st:
+        st.ingest(hg)
+        for l in (0, 7):
+            with st.snapshot(l) as sn:
+                r = sn.triangle_count()
+                assert r.triangles == O.tc(l)
+                assert r.arcs == sn.num_edges
