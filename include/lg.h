@@ -291,6 +291,71 @@ typedef struct lg_tc_result {
 
 lg_status lg_triangle_count(lg_snapshot* snap, lg_tc_result* result);
 
+/* Strongly connected components: task "tarjan_scc" (ll_b_tarjan_scc,
+ * benchmark/benchmarks/tarjan_scc.h:121-206).  The reference's Green-Marl
+ * Tarjan uses vertex ids as low-links and does not return true SCCs; this
+ * call returns the true partition, each component labelled by its smallest
+ * vertex id.  labels: int64[max_nodes].  Requires the in-CSR.  result (may be
+ * NULL): number of components, vertices trimmed as singletons up front,
+ * colouring rounds and traversal steps. */
+typedef struct lg_scc_result {
+	uint64_t components;
+	uint64_t trimmed;
+	int32_t  rounds;
+	int32_t  steps;
+} lg_scc_result;
+
+lg_status lg_scc(lg_snapshot* snap, int64_t* labels, lg_scc_result* result);
+
+/* Brandes betweenness centrality from explicit sources: the kernel of task
+ * "bc_random" (ll_b_bc_random::run, benchmark/benchmarks/bc_random.h:158-193,
+ * bc_random_bfs :55-116) with the sources given instead of drawn by
+ * pick_random_node(), accumulated in FP64 (the reference uses FP32).
+ * Directed, no halving; BC[v] += delta_s[v] for v != s.  bc: double[max_nodes].
+ * lg_bc runs one source after another; lg_bc_batched runs 64 sources per
+ * pass (one edge traversal serves 64 BFSs) and returns the same values up to
+ * FP64 summation order. */
+lg_status lg_bc(lg_snapshot* snap, const int64_t* sources, int n_sources,
+		double* bc);
+lg_status lg_bc_batched(lg_snapshot* snap, const int64_t* sources, int n_sources,
+		double* bc);
+
+/* Personalized PageRank for K single-vertex seeds, evaluated on n_snaps
+ * snapshots of one store in a single CUDA-graph launch.  The reference has no
+ * personalized variant: this is the pull iteration of pagerank_double
+ * (benchmark/benchmarks/pagerank.h:120-169) with the uniform teleport
+ * (1-d)/N replaced, per column k, by (1-d) on seed k; x0 = e_seed, fixed
+ * iteration count, dangling mass dropped.  K is a multiple of 32, <= 256.
+ * out: double[n_snaps][max_nodes][K] (row-major, column k = seed k). */
+lg_status lg_ppr(lg_snapshot* const* snaps, int n_snaps, const int64_t* seeds,
+		int K, int iterations, double damping, double* out);
+
+/* Differentiable weighted PageRank (no reference counterpart; the pull
+ * iteration of pagerank.h:120-169 with per-edge weights and a teleport
+ * vector).  Forward: x = (1-d) teleport + d P^T x from x = teleport until
+ * sum |x' - x| < tol (or max_iter), P(w->t) = weights[p] where p is the
+ * edge's position in the snapshot's out-adjacency order (lg_snapshot_adjacency
+ * dir 0); the caller normalises rows if it wants a stochastic P.  x:
+ * double[max_nodes].  If tape is non-NULL the converged x is kept for
+ * lg_pagerank_bwd, which solves the transposed fixed point
+ * lambda = dL/dx + d P lambda (implicit differentiation, no stored iterates)
+ * and returns dL/dweights (double[num_edges], same order) = d lambda[t] x[w]
+ * and dL/dteleport (double[max_nodes]) = (1-d) lambda; either may be NULL.
+ * Free the tape with lg_adjoint_free before closing the snapshot. */
+typedef struct lg_adjoint lg_adjoint;
+typedef struct lg_fixed_point_result {
+	int32_t iterations;
+	int32_t reserved;
+	double  residual;   /* sum |x' - x| of the last iteration */
+} lg_fixed_point_result;
+
+lg_status lg_pagerank_fwd(lg_snapshot* snap, const double* weights,
+		const double* teleport, double damping, double tol, int max_iter,
+		double* x, lg_adjoint** tape, lg_fixed_point_result* result);
+lg_status lg_pagerank_bwd(lg_adjoint* tape, const double* dldx, double* dldw,
+		double* dldteleport, lg_fixed_point_result* result);
+lg_status lg_adjoint_free(lg_adjoint* tape);
+
 /* ---------------------------------------------------------------------------
  * Errors.
  * ------------------------------------------------------------------------- */

@@ -80,6 +80,16 @@ class lg_tc_result(C.Structure):
                 ("arcs", C.c_uint64)]
 
 
+class lg_scc_result(C.Structure):
+    _fields_ = [("components", C.c_uint64), ("trimmed", C.c_uint64),
+                ("rounds", C.c_int32), ("steps", C.c_int32)]
+
+
+class lg_fixed_point_result(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("reserved", C.c_int32),
+                ("residual", C.c_double)]
+
+
 class lg_snapshot_stats(C.Structure):
     _fields_ = [("max_nodes", C.c_uint64), ("live_edges", C.c_uint64),
                 ("slots", C.c_uint64), ("fragment_slots", C.c_uint64),
@@ -130,6 +140,14 @@ SIGNATURES = [
     ("lg_bfs", _INT, [_P, _I64, _P, C.POINTER(lg_bfs_result)]),
     ("lg_sssp_delta", _INT, [_P, _I64, C.c_uint32, _P, C.POINTER(lg_sssp_result)]),
     ("lg_triangle_count", _INT, [_P, C.POINTER(lg_tc_result)]),
+    ("lg_scc", _INT, [_P, _P, C.POINTER(lg_scc_result)]),
+    ("lg_bc", _INT, [_P, _P, _INT, _P]),
+    ("lg_bc_batched", _INT, [_P, _P, _INT, _P]),
+    ("lg_ppr", _INT, [_P, _INT, _P, _INT, _INT, _D, _P]),
+    ("lg_pagerank_fwd", _INT, [_P, _P, _P, _D, _D, _INT, _P, _PP,
+                               C.POINTER(lg_fixed_point_result)]),
+    ("lg_pagerank_bwd", _INT, [_P, _P, _P, _P, C.POINTER(lg_fixed_point_result)]),
+    ("lg_adjoint_free", _INT, [_P]),
     ("lg_last_error", C.c_size_t, [C.c_char_p, C.c_size_t]),
     ("lg_status_string", C.c_char_p, [_INT]),
     ("lg_version", C.c_char_p, []),

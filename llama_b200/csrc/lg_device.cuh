@@ -205,8 +205,14 @@ struct lg_store {
 	uint64_t d2h_bytes = 0;     // device -> host bytes copied by this store
 };
 
+// Edge-order maps of a snapshot used by the differentiable PageRank
+// (lg_adjoint.cu); built on first use, freed with the snapshot.
+struct lg_adjoint_maps;
+void lg_free_adjoint_maps(lg_adjoint_maps* m);
+
 struct lg_snapshot {
 	lg_store* store = nullptr;
+	lg_adjoint_maps* adj_maps = nullptr;
 	int level = 0;
 	uint64_t V = 0;
 	lg::SnapDir out, in;

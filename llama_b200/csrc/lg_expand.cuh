@@ -126,6 +126,61 @@ __device__ __forceinline__ void range_entries(const uint32_t* pos, uint32_t n,
 	*e_end = last_range ? n : warp_lower_bound(pos, n, b);
 }
 
+// Process range `r` of a list's slot space (ranges of `range` slots, nranges
+// of them, `total` slots) and call, for every chunk of 32 slots and on all 32
+// lanes, body(active, owner_lane, owner_vertex, nbr, level, index) - active =
+// the lane holds a live slot.  The body may use warp collectives.  Owner
+// lanes are non-decreasing across a chunk and lanes past the window's last
+// slot get owner lane 31, so owner_lane is a safe key for segmented
+// reductions (owner_vertex of such lanes is a placeholder).
+template <class Body>
+__device__ __forceinline__ void range_for_each(const SnapCsr& g, const uint32_t* list,
+		const uint32_t* pos, uint32_t n, uint32_t total, uint32_t nranges,
+		uint32_t range, uint32_t r, Body&& body) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const bool last_range = r == nranges - 1;
+	const uint32_t ra = r * range;
+	const uint32_t rb = last_range ? total : min(total, ra + range);
+	uint32_t e_begin, e_end;
+	range_entries(pos, n, ra, rb, last_range, &e_begin, &e_end);
+	const LevelTab* lt = g.lt;
+	for (uint32_t ew = e_begin; ew < e_end; ew += 32) {
+		const Window w = load_window(g, list, pos, ew, e_end, ra, rb);
+		for (uint32_t base = w.lo; base < w.hi; base += 32 * kUnroll) {
+			uint32_t nb[kUnroll], own[kUnroll], lvs[kUnroll], ids[kUnroll];
+			bool act[kUnroll];
+#pragma unroll
+			for (int u = 0; u < kUnroll; u++) {
+				const uint32_t k = base + u * 32 + lane;
+				locate_slot(g, w, k, &own[u], &lvs[u], &ids[u]);
+				act[u] = k < w.hi;
+				nb[u] = 0;
+				if (act[u]) {
+					const uint32_t word = __ldg(lt->del[lvs[u]] + (ids[u] >> 5));
+					nb[u] = __ldg(lt->ids[lvs[u]] + ids[u]);
+					act[u] = !((word >> (ids[u] & 31)) & 1u);
+				}
+			}
+#pragma unroll
+			for (int u = 0; u < kUnroll; u++) {
+				const uint32_t ov = __shfl_sync(0xffffffffu, w.v, own[u]);
+				body(act[u], own[u], ov, nb[u], lvs[u], ids[u]);
+			}
+		}
+	}
+	(void)lane;
+}
+
+// Frontier bookkeeping shared by the list-driven kernels: per-entry slot
+// counts, to be scanned into the `pos` offsets range_for_each expects.
+static __global__ void list_slots(SnapCsr g, const uint32_t* list, uint32_t n,
+		uint32_t* cnt) {
+	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= n) return;
+	uint32_t f0;
+	cnt[i] = vertex_slots(g, list ? __ldg(list + i) : (uint32_t)i, &f0);
+}
+
 } // namespace lg
 
 #endif // LG_EXPAND_CUH_

@@ -49,9 +49,92 @@ __device__ __forceinline__ void pr_finish(const PrArgs& a, uint32_t v, double s)
 	if (a.pr_out) a.pr_out[v] = pr;
 }
 
+// Sum of contrib over `n` slots of a vertex's fragment chain, starting `off`
+// slots into it, by one lane in iteration order (4 loads in flight).
+__device__ __forceinline__ double lane_sum(const PrArgs& a, uint32_t f, uint32_t off,
+		uint32_t n) {
+	const LevelTab* lt = a.in.lt;
+	uint2 fr = a.in.frags[f];
+	while (off >= frag_len(fr)) { off -= frag_len(fr); fr = a.in.frags[++f]; }
+	double s = 0.0;
+	while (n > 0) {
+		const uint32_t lv = frag_level(fr);
+		const uint32_t base = fr.x + off;
+		const uint32_t m = min(frag_len(fr) - off, n);
+		const uint32_t* ids = lt->ids[lv] + base;
+		const uint32_t* del = lt->del[lv];
+		uint32_t i = 0;
+		for (; i + 4 <= m; i += 4) {
+			uint32_t id[4], dw[4];
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				id[u] = __ldg(ids + i + u);
+				dw[u] = __ldg(del + ((base + i + u) >> 5));
+			}
+			double x[4];
+#pragma unroll
+			for (int u = 0; u < 4; u++)
+				x[u] = ((dw[u] >> ((base + i + u) & 31)) & 1u) ? 0.0 : __ldg(a.contrib + id[u]);
+#pragma unroll
+			for (int u = 0; u < 4; u++) s += x[u];
+		}
+		for (; i < m; i++) {
+			const uint32_t dw = __ldg(del + ((base + i) >> 5));
+			if (!((dw >> ((base + i) & 31)) & 1u)) s += __ldg(a.contrib + __ldg(ids + i));
+		}
+		n -= m;
+		off = 0;
+		if (n) fr = a.in.frags[++f];
+	}
+	return s;
+}
+
+// Sum over `n` slots of one vertex (starting `off` slots in) by the whole
+// warp: lane i takes slots i, i + 32, ..., then a fixed tree reduction.
+__device__ __forceinline__ double warp_sum(const PrArgs& a, uint32_t f, uint32_t off,
+		uint32_t n) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const LevelTab* lt = a.in.lt;
+	uint2 fr = a.in.frags[f];
+	while (off >= frag_len(fr)) { off -= frag_len(fr); fr = a.in.frags[++f]; }
+	double s = 0.0;
+	while (n > 0) {
+		const uint32_t lv = frag_level(fr);
+		const uint32_t base = fr.x + off;
+		const uint32_t m = min(frag_len(fr) - off, n);
+		const uint32_t* ids = lt->ids[lv] + base;
+		const uint32_t* del = lt->del[lv];
+		for (uint32_t i0 = 0; i0 < m; i0 += 32 * kUnroll) {
+			uint32_t id[kUnroll];
+			bool live[kUnroll];
+#pragma unroll
+			for (int u = 0; u < kUnroll; u++) {
+				const uint32_t i = i0 + u * 32 + lane;
+				live[u] = i < m;
+				id[u] = 0;
+				if (live[u]) {
+					const uint32_t dw = __ldg(del + ((base + i) >> 5));
+					id[u] = __ldg(ids + i);
+					live[u] = !((dw >> ((base + i) & 31)) & 1u);
+				}
+			}
+#pragma unroll
+			for (int u = 0; u < kUnroll; u++) if (live[u]) s += __ldg(a.contrib + id[u]);
+		}
+		n -= m;
+		off = 0;
+		if (n) fr = a.in.frags[++f];
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+	return s;
+}
+
+// One warp per range of kPrRange slots.  Entries (vertices) with fewer than
+// 32 slots in the range are summed by their own lane, sequentially in
+// iteration order; longer ones by the whole warp.
 __global__ void __launch_bounds__(kPrThreads)
 pr_pull_step(PrArgs a) {
-	__shared__ double acc[kPrWarps][32];
 	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
 	const uint64_t r64 = (uint64_t)blockIdx.x * kPrWarps + wid;
 	if (r64 >= a.nranges) return;
@@ -61,46 +144,26 @@ pr_pull_step(PrArgs a) {
 	const uint32_t rb = last_range ? a.total : min(a.total, ra + kPrRange);
 	uint32_t e_begin, e_end;
 	range_entries(a.pos, (uint32_t)a.in.V, ra, rb, last_range, &e_begin, &e_end);
-	const LevelTab* lt = a.in.lt;
 	for (uint32_t ew = e_begin; ew < e_end; ew += 32) {
 		const Window w = load_window(a.in, nullptr, a.pos, ew, e_end, ra, rb);
-		acc[wid][lane] = 0.0;
-		__syncwarp();
-		for (uint32_t base = w.lo; base < w.hi; base += 32 * kUnroll) {
-			uint32_t own[kUnroll], nb[kUnroll];
-			bool act[kUnroll];
-#pragma unroll
-			for (int u = 0; u < kUnroll; u++) {
-				const uint32_t k = base + u * 32 + lane;
-				uint32_t lv, idx;
-				locate_slot(a.in, w, k, &own[u], &lv, &idx);
-				act[u] = k < w.hi;
-				nb[u] = 0;
-				if (act[u]) {
-					const uint32_t word = __ldg(lt->del[lv] + (idx >> 5));
-					nb[u] = __ldg(lt->ids[lv] + idx);
-					act[u] = !((word >> (idx & 31)) & 1u);
-				}
-			}
-			double x[kUnroll];
-#pragma unroll
-			for (int u = 0; u < kUnroll; u++) x[u] = act[u] ? __ldg(a.contrib + nb[u]) : 0.0;
-#pragma unroll
-			for (int u = 0; u < kUnroll; u++) {
-				bool tail;
-				const double s = warp_segsum(x[u], own[u], &tail);
-				if (tail) acc[wid][own[u]] += s;
-				__syncwarp();
-			}
+		const uint32_t span = w.s1 - w.s0;
+		const bool longe = w.valid && span >= 32;
+		double s = 0.0;
+		if (w.valid && !longe && span > 0) s = lane_sum(a, w.f0, w.s0 - w.start, span);
+		for (unsigned m = __ballot_sync(0xffffffffu, longe); m; m &= m - 1) {
+			const int t = __ffs(m) - 1;
+			const uint32_t f0 = __shfl_sync(0xffffffffu, w.f0, t);
+			const uint32_t off = __shfl_sync(0xffffffffu, w.s0 - w.start, t);
+			const uint32_t n = __shfl_sync(0xffffffffu, span, t);
+			const double ws = warp_sum(a, f0, off, n);
+			if ((int)lane == t) s = ws;
 		}
 		if (w.valid) {
-			const double s = acc[wid][lane];
 			const uint32_t end = __ldg(a.pos + w.e + 1);
 			if (w.start < ra) a.carry_first[r] = s;        // began before the range
 			else if (end > rb) a.carry_last[r] = s;        // runs past its end
 			else pr_finish(a, w.v, s);
 		}
-		__syncwarp();
 	}
 }
 

@@ -759,6 +759,7 @@ lg_status lg_snapshot_close(lg_snapshot* sn) {
 	cudaSetDevice(sn->store->device);
 	cudaStreamSynchronize(sn->store->stream);
 	sn->store->open_snapshots--;
+	if (sn->adj_maps) lg_free_adjoint_maps(sn->adj_maps);
 	delete sn;
 	return LG_OK;
 }

@@ -189,6 +189,45 @@ class Store:
         return Snapshot(self, level)
 
 
+class Tape:
+    """Converged scores of a lg_pagerank_fwd call, for lg_pagerank_bwd."""
+
+    def __init__(self, handle, snapshot):
+        self._h = handle
+        self.snapshot = snapshot
+
+    def backward(self, dldx, dldw=None, dldv=None):
+        """Returns (dL/dweights, dL/dteleport, result)."""
+        g = np.ascontiguousarray(dldx, np.float64) if not hasattr(dldx, "data_ptr") else dldx
+        if dldw is None:
+            dldw = np.empty(self.snapshot.num_edges, np.float64)
+        if dldv is None:
+            dldv = np.empty(self.snapshot.max_nodes, np.float64)
+        r = _lib.lg_fixed_point_result()
+        check(lib.lg_pagerank_bwd(self._h, ptr(g), ptr(dldw), ptr(dldv), C.byref(r)))
+        return dldw, dldv, r
+
+    def close(self):
+        if self._h:
+            lib.lg_adjoint_free(self._h)
+            self._h = None
+
+    __del__ = close
+
+
+def ppr(snapshots, seeds, iterations=20, damping=0.85, out=None):
+    """Personalized PageRank (``lg_ppr``) for len(seeds) seeds on every
+    snapshot in one captured graph; returns [n_snaps, max_nodes, K]."""
+    snaps = list(snapshots)
+    arr = (C.c_void_p * len(snaps))(*[s.handle.value for s in snaps])
+    s = np.ascontiguousarray(seeds, np.int64)
+    V = snaps[0].max_nodes
+    res = np.empty((len(snaps), V, len(s)), np.float64) if out is None else out
+    check(lib.lg_ppr(C.cast(arr, C.c_void_p), len(snaps), ptr(s), len(s), int(iterations),
+                     float(damping), ptr(res)))
+    return res
+
+
 class Snapshot:
     """Read-only view of one level (``lg_snapshot``)."""
 
@@ -264,6 +303,36 @@ class Snapshot:
         r = _lib.lg_bfs_result()
         check(lib.lg_bfs(self._h, int(root), ptr(res), C.byref(r)))
         return res, r
+
+    def scc(self, out=None):
+        """Strongly connected components, labelled by their smallest vertex;
+        returns (labels, lg_scc_result)."""
+        res = np.empty(self.max_nodes, np.int64) if out is None else out
+        r = _lib.lg_scc_result()
+        check(lib.lg_scc(self._h, ptr(res), C.byref(r)))
+        return res, r
+
+    def bc(self, sources, batched=True, out=None):
+        """Brandes BC from `sources` (FP64); batched = 64 sources per pass."""
+        src = np.ascontiguousarray(sources, np.int64)
+        res = np.empty(self.max_nodes, np.float64) if out is None else out
+        fn = lib.lg_bc_batched if batched else lib.lg_bc
+        check(fn(self._h, ptr(src), len(src), ptr(res)))
+        return res
+
+    def pagerank_fwd(self, weights, teleport, damping=0.85, tol=1e-12, max_iter=10000,
+                     keep_tape=True, out=None):
+        """Weighted PageRank fixed point (``lg_pagerank_fwd``); weights follow
+        the out-adjacency order.  Returns (x, Tape or None, result)."""
+        w = np.ascontiguousarray(weights, np.float64) if not hasattr(weights, "data_ptr") else weights
+        v = np.ascontiguousarray(teleport, np.float64) if not hasattr(teleport, "data_ptr") else teleport
+        x = np.empty(self.max_nodes, np.float64) if out is None else out
+        t = C.c_void_p()
+        r = _lib.lg_fixed_point_result()
+        check(lib.lg_pagerank_fwd(self._h, ptr(w), ptr(v), float(damping), float(tol),
+                                  int(max_iter), ptr(x), C.byref(t) if keep_tape else None,
+                                  C.byref(r)))
+        return x, (Tape(t, self) if keep_tape else None), r
 
     def triangle_count(self):
         """Task ``tc_u`` on the symmetrised snapshot; returns lg_tc_result."""

@@ -50,6 +50,8 @@ def lgo():
             ("lgo_tc", _I64, [_P, _INT]),
             ("lgo_scc", None, [_P, _INT, _P]),
             ("lgo_ppr", None, [_P, _INT, _P, _INT, _INT, _D, _P]),
+            ("lgo_wpr_forward", _INT, [_P, _INT, _P, _P, _D, _D, _INT, _P]),
+            ("lgo_wpr_backward", _INT, [_P, _INT, _P, _P, _P, _D, _D, _INT, _P, _P]),
         ]:
             f = getattr(L, name)
             f.restype, f.argtypes = res, args
@@ -176,6 +178,23 @@ class Oracle(_Base):
         out = np.empty(self.V, np.int64)
         lgo().lgo_scc(self.h, level, _p(out))
         return out
+
+    def wpr_forward(self, level, weights, teleport, damping=0.85, tol=1e-12, max_iter=10000):
+        w = np.ascontiguousarray(weights, np.float64)
+        v = np.ascontiguousarray(teleport, np.float64)
+        x = np.empty(self.V, np.float64)
+        it = lgo().lgo_wpr_forward(self.h, level, _p(w), _p(v), damping, tol, max_iter, _p(x))
+        return x, it
+
+    def wpr_backward(self, level, weights, x, dldx, damping=0.85, tol=1e-12, max_iter=10000):
+        w = np.ascontiguousarray(weights, np.float64)
+        xx = np.ascontiguousarray(x, np.float64)
+        g = np.ascontiguousarray(dldx, np.float64)
+        dw = np.empty(len(w), np.float64)
+        dv = np.empty(self.V, np.float64)
+        it = lgo().lgo_wpr_backward(self.h, level, _p(w), _p(xx), _p(g), damping, tol,
+                                    max_iter, _p(dw), _p(dv))
+        return dw, dv, it
 
     def ppr(self, level, seeds, iterations, damping=0.85):
         s = np.ascontiguousarray(seeds, np.int64)

@@ -546,6 +546,65 @@ void lgo_scc(void* gp, int level, int64_t* label) {
 	}
 }
 
+// Weighted PageRank to a fixed point (no reference counterpart; the pull
+// iteration of pagerank.h:120-169 with per-edge weights and a teleport
+// vector): x' = (1-d) v + d P^T x, P(w->t) = weight of the out-edge, given in
+// the snapshot's out-adjacency iteration order.  Starts at x = v, stops when
+// sum |x' - x| < tol.  Returns the number of iterations.
+int lgo_wpr_forward(void* gp, int level, const double* w, const double* v, double d,
+		double tol, int max_iter, double* x) {
+	Graph* g = (Graph*)gp;
+	const uint64_t V = g->V;
+	std::vector<std::vector<uint32_t>> out(V);
+	for (uint64_t u = 0; u < V; u++) neighbours(g->out, level, u, out[u], nullptr);
+	std::vector<double> nx(V);
+	for (uint64_t t = 0; t < V; t++) x[t] = v[t];
+	int it = 0;
+	while (it < max_iter) {
+		for (uint64_t t = 0; t < V; t++) nx[t] = (1 - d) * v[t];
+		uint64_t p = 0;
+		for (uint64_t u = 0; u < V; u++)
+			for (uint32_t t : out[u]) nx[t] += d * (w[p++] * x[u]);
+		double r = 0;
+		for (uint64_t t = 0; t < V; t++) { r += std::fabs(nx[t] - x[t]); x[t] = nx[t]; }
+		it++;
+		if (r < tol) break;
+	}
+	return it;
+}
+
+// Adjoint of lgo_wpr_forward by implicit differentiation: with
+// g = dL/dx, lambda solves lambda = g + d P lambda (the transposed fixed
+// point, iterated over out-edges), and dL/dv = (1-d) lambda,
+// dL/dP(w->t) = d lambda[t] x[w].  Returns the number of iterations.
+int lgo_wpr_backward(void* gp, int level, const double* w, const double* x,
+		const double* gv, double d, double tol, int max_iter, double* dldw,
+		double* dldv) {
+	Graph* g = (Graph*)gp;
+	const uint64_t V = g->V;
+	std::vector<std::vector<uint32_t>> out(V);
+	for (uint64_t u = 0; u < V; u++) neighbours(g->out, level, u, out[u], nullptr);
+	std::vector<double> lam(gv, gv + V), nl(V);
+	int it = 0;
+	while (it < max_iter) {
+		uint64_t p = 0;
+		double r = 0;
+		for (uint64_t u = 0; u < V; u++) {
+			double s = 0;
+			for (uint32_t t : out[u]) s += w[p++] * lam[t];
+			nl[u] = gv[u] + d * s;
+		}
+		for (uint64_t u = 0; u < V; u++) { r += std::fabs(nl[u] - lam[u]); lam[u] = nl[u]; }
+		it++;
+		if (r < tol) break;
+	}
+	uint64_t p = 0;
+	for (uint64_t u = 0; u < V; u++)
+		for (uint32_t t : out[u]) dldw[p++] = d * lam[t] * x[u];
+	for (uint64_t t = 0; t < V; t++) dldv[t] = (1 - d) * lam[t];
+	return it;
+}
+
 // Personalized PageRank with K single-vertex teleport seeds, the pull
 // iteration of pagerank.h:120-169 with the uniform teleport (1-d)/N replaced
 // by (1-d) * [t == seed_k]: x0 = e_seed, then `iters` times

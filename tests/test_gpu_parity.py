@@ -222,3 +222,92 @@ def test_triangles_multiversion_vs_oracle():
                 r = sn.triangle_count()
                 assert r.triangles == O.tc(l)
                 assert r.arcs == sn.num_edges
+
+
+def test_golden_scc(golden):
+    V = int(golden["V"])
+    hg, st = device_store(golden["levels"], V)
+    with st:
+        for l in range(len(golden["levels"])):
+            with st.snapshot(l) as sn:
+                lab, res = sn.scc()
+                assert np.array_equal(lab, golden[f"scc{l}"]), l
+                assert res.components == len(np.unique(lab))
+
+
+def test_scc_multiversion_vs_oracle():
+    spec = workloads.rmat_multiversion(scale=15, seed=9, levels=4, level0=0.8, delete=0.02)
+    hg = HostGraph.from_spec(spec)
+    O = _oracle_for(hg)
+    with Store() as st:
+        st.ingest(hg)
+        for l in (1, 3):
+            with st.snapshot(l) as sn:
+                lab, _ = sn.scc()
+                assert np.array_equal(lab, O.scc(l))
+
+
+BC_TOL = 1e-9
+
+
+def _bc_close(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.all(np.abs(a - b) <= BC_TOL * np.maximum(np.abs(b), 1.0))
+
+
+def test_golden_bc_plain_and_batched(golden):
+    """FP64 BC vs the FP64 oracle (1e-9) and the FP32 reference (1e-5)."""
+    V = int(golden["V"])
+    hg, st = device_store(golden["levels"], V)
+    O = Oracle(V)
+    O.add_levels(golden["levels"])
+    src = golden["bc_sources"]
+    with st:
+        for l in range(len(golden["levels"])):
+            with st.snapshot(l) as sn:
+                ref = O.bc(l, src)
+                plain = sn.bc(src, batched=False)
+                batched = sn.bc(src, batched=True)
+                assert _bc_close(plain, ref), l
+                assert _bc_close(batched, ref), l
+                f32 = golden[f"bc{l}"].astype(np.float64)
+                assert np.all(np.abs(batched - f32) <= 1e-5 * np.maximum(np.abs(batched), 1.0))
+
+
+def test_bc_batched_many_sources_vs_oracle():
+    """More than one 64-source batch, repeated sources, a symmetric graph."""
+    spec = workloads.kronecker_symmetric(scale=11, seed=6, levels=4)
+    hg = HostGraph.from_spec(spec)
+    O = _oracle_for(hg)
+    with Store() as st:
+        st.ingest(hg)
+        with st.snapshot() as sn:
+            src = workloads.pick_roots(sn.out_degrees(), 100, seed=7)
+            src = np.concatenate([src, src[:5]])
+            ref = O.bc(3, src)
+            assert _bc_close(sn.bc(src, batched=True), ref)
+            assert _bc_close(sn.bc(src[:20], batched=False), O.bc(3, src[:20]))
+
+
+def test_ppr_block_all_snapshots_vs_oracle():
+    from llama_b200.graph import ppr
+    spec = workloads.kronecker_symmetric(scale=11, seed=6, levels=4)
+    hg = HostGraph.from_spec(spec)
+    O = _oracle_for(hg)
+    with Store() as st:
+        st.ingest(hg)
+        snaps = [st.snapshot(l) for l in range(4)]
+        try:
+            seeds = workloads.pick_roots(snaps[-1].out_degrees(), 64, seed=11)
+            seeds[3] = seeds[7]                       # a repeated seed
+            res = ppr(snaps, seeds, iterations=6)
+            for l in range(4):
+                ref = O.ppr(l, seeds, 6)
+                den = np.maximum(np.abs(ref), 1e-300)
+                assert np.max(np.abs(res[l] - ref) / den) <= 1e-12, l
+            # K = 32 path and iteration count 0
+            r0 = ppr(snaps[:1], seeds[:32], iterations=0)
+            assert np.array_equal(r0[0], O.ppr(0, seeds[:32], 0))
+        finally:
+            for s in snaps:
+                s.close()
