@@ -9,23 +9,32 @@
 // loads in the reference), each iteration writes contrib'[t] = pr'[t] /
 // out_degree(t), so an edge costs one 4-byte id load and one 8-byte gather.
 // The division is the one the reference performs per edge, so the gathered
-// values are bit-identical; only the summation order differs (FP64, well
-// within 1e-12).
+// values are bit-identical; a vertex's sum is taken in the reference's
+// iteration order except where it is split across blocks (FP64, well within
+// 1e-12 in every case).
 //
-// Work split (lg_expand.cuh): the in-CSR slot space of all vertices, in
-// vertex order, is cut into ranges of kPrRange slots, one warp per range.  A
-// vertex whose slots straddle range boundaries leaves one partial sum per
-// range (carry_first: it began before the range, carry_last: it runs past
-// the end) and pr_fixup adds those partials in range order, so every result
-// is deterministic.
+// Work split: the in-CSR slot space of all vertices (vertex order, each
+// vertex's fragments newest first) is cut into blocks of kPrRange slots, one
+// CTA each.  Phase 1 streams the block's slots: every thread takes
+// kPrPerThread slots, finds each slot's fragment by binary search in a
+// shared-memory table of the block's fragments, and issues all its id,
+// deletion-word and contrib loads before using any of them, so a CTA keeps
+// 2048 gathers in flight.  The values land in shared memory.  Phase 2 sums
+// each vertex's values from shared memory (one thread per short vertex, a
+// warp per long one).  A vertex whose slots straddle blocks leaves one
+// partial per block (carry_first: it began before the block, carry_last: it
+// runs past its end) and pr_fixup adds them in block order, so results are
+// deterministic.
 #include "lg_device.cuh"
 #include "lg_expand.cuh"
 
 namespace lg {
 
-constexpr uint32_t kPrRange = 2048;
 constexpr int kPrThreads = 256;
-constexpr int kPrWarps = kPrThreads / 32;
+constexpr int kPrPerThread = 8;
+constexpr uint32_t kPrRange = kPrThreads * kPrPerThread;        // 2048 slots
+constexpr uint32_t kPrMaxFrags = kPrRange + 2 * LG_MAX_LEVELS;   // fragments touching a block
+constexpr uint32_t kPrLong = 64;       // entries with more slots are reduced by a warp
 
 struct PrArgs {
 	SnapCsr in;
@@ -38,8 +47,8 @@ struct PrArgs {
 	double* pr_out;            // written when non-null (last iteration)
 	double base;               // (1 - d) / N
 	double d;
-	double* carry_first;       // per range
-	double* carry_last;        // per range
+	double* carry_first;       // per block
+	double* carry_last;        // per block
 };
 
 __device__ __forceinline__ void pr_finish(const PrArgs& a, uint32_t v, double s) {
@@ -49,126 +58,129 @@ __device__ __forceinline__ void pr_finish(const PrArgs& a, uint32_t v, double s)
 	if (a.pr_out) a.pr_out[v] = pr;
 }
 
-// Sum of contrib over `n` slots of a vertex's fragment chain, starting `off`
-// slots into it, by one lane in iteration order (4 loads in flight).
-__device__ __forceinline__ double lane_sum(const PrArgs& a, uint32_t f, uint32_t off,
-		uint32_t n) {
-	const LevelTab* lt = a.in.lt;
-	uint2 fr = a.in.frags[f];
-	while (off >= frag_len(fr)) { off -= frag_len(fr); fr = a.in.frags[++f]; }
-	double s = 0.0;
-	while (n > 0) {
-		const uint32_t lv = frag_level(fr);
-		const uint32_t base = fr.x + off;
-		const uint32_t m = min(frag_len(fr) - off, n);
-		const uint32_t* ids = lt->ids[lv] + base;
-		const uint32_t* del = lt->del[lv];
-		uint32_t i = 0;
-		for (; i + 4 <= m; i += 4) {
-			uint32_t id[4], dw[4];
-#pragma unroll
-			for (int u = 0; u < 4; u++) {
-				id[u] = __ldg(ids + i + u);
-				dw[u] = __ldg(del + ((base + i + u) >> 5));
-			}
-			double x[4];
-#pragma unroll
-			for (int u = 0; u < 4; u++)
-				x[u] = ((dw[u] >> ((base + i + u) & 31)) & 1u) ? 0.0 : __ldg(a.contrib + id[u]);
-#pragma unroll
-			for (int u = 0; u < 4; u++) s += x[u];
-		}
-		for (; i < m; i++) {
-			const uint32_t dw = __ldg(del + ((base + i) >> 5));
-			if (!((dw >> ((base + i) & 31)) & 1u)) s += __ldg(a.contrib + __ldg(ids + i));
-		}
-		n -= m;
-		off = 0;
-		if (n) fr = a.in.frags[++f];
-	}
-	return s;
+__device__ __forceinline__ void pr_emit(const PrArgs& a, uint32_t r, uint32_t ra, uint32_t rb,
+		uint32_t e, uint32_t start, uint32_t end, double s) {
+	if (start < ra) a.carry_first[r] = s;          // began before the block
+	else if (end > rb) a.carry_last[r] = s;        // runs past its end
+	else pr_finish(a, e, s);
 }
 
-// Sum over `n` slots of one vertex (starting `off` slots in) by the whole
-// warp: lane i takes slots i, i + 32, ..., then a fixed tree reduction.
-__device__ __forceinline__ double warp_sum(const PrArgs& a, uint32_t f, uint32_t off,
-		uint32_t n) {
-	const uint32_t lane = threadIdx.x & 31u;
-	const LevelTab* lt = a.in.lt;
-	uint2 fr = a.in.frags[f];
-	while (off >= frag_len(fr)) { off -= frag_len(fr); fr = a.in.frags[++f]; }
-	double s = 0.0;
-	while (n > 0) {
-		const uint32_t lv = frag_level(fr);
-		const uint32_t base = fr.x + off;
-		const uint32_t m = min(frag_len(fr) - off, n);
-		const uint32_t* ids = lt->ids[lv] + base;
-		const uint32_t* del = lt->del[lv];
-		for (uint32_t i0 = 0; i0 < m; i0 += 32 * kUnroll) {
-			uint32_t id[kUnroll];
-			bool live[kUnroll];
-#pragma unroll
-			for (int u = 0; u < kUnroll; u++) {
-				const uint32_t i = i0 + u * 32 + lane;
-				live[u] = i < m;
-				id[u] = 0;
-				if (live[u]) {
-					const uint32_t dw = __ldg(del + ((base + i) >> 5));
-					id[u] = __ldg(ids + i);
-					live[u] = !((dw >> ((base + i) & 31)) & 1u);
-				}
-			}
-#pragma unroll
-			for (int u = 0; u < kUnroll; u++) if (live[u]) s += __ldg(a.contrib + id[u]);
-		}
-		n -= m;
-		off = 0;
-		if (n) fr = a.in.frags[++f];
-	}
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-	return s;
-}
-
-// One warp per range of kPrRange slots.  Entries (vertices) with fewer than
-// 32 slots in the range are summed by their own lane, sequentially in
-// iteration order; longer ones by the whole warp.
 __global__ void __launch_bounds__(kPrThreads)
 pr_pull_step(PrArgs a) {
-	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-	const uint64_t r64 = (uint64_t)blockIdx.x * kPrWarps + wid;
-	if (r64 >= a.nranges) return;
-	const uint32_t r = (uint32_t)r64;
+	__shared__ double vals[kPrRange];
+	__shared__ uint2 ftab[kPrMaxFrags];
+	__shared__ uint32_t fstart[kPrMaxFrags + 1];
+	__shared__ uint32_t longs[kPrRange / kPrLong + 2];
+	__shared__ uint32_t sh_eb, sh_ee, sh_nlong;
+	__shared__ uint32_t wsum[kPrThreads / 32];
+	const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
+	const uint32_t r = blockIdx.x;
 	const bool last_range = r == a.nranges - 1;
 	const uint32_t ra = r * kPrRange;
 	const uint32_t rb = last_range ? a.total : min(a.total, ra + kPrRange);
-	uint32_t e_begin, e_end;
-	range_entries(a.pos, (uint32_t)a.in.V, ra, rb, last_range, &e_begin, &e_end);
-	for (uint32_t ew = e_begin; ew < e_end; ew += 32) {
-		const Window w = load_window(a.in, nullptr, a.pos, ew, e_end, ra, rb);
-		const uint32_t span = w.s1 - w.s0;
-		const bool longe = w.valid && span >= 32;
+	if (wid == 0) {
+		uint32_t eb, ee;
+		range_entries(a.pos, (uint32_t)a.in.V, ra, rb, last_range, &eb, &ee);
+		if (lane == 0) { sh_eb = eb; sh_ee = ee; sh_nlong = 0; }
+	}
+	__syncthreads();
+	const uint32_t eb = sh_eb, ee = sh_ee;
+
+	// fragment table of the block's entries, with absolute virtual starts
+	const uint32_t f_begin = __ldg(a.in.frag_off + eb);
+	uint32_t nf = (ee > eb) ? __ldg(a.in.frag_off + ee) - f_begin : 0;
+	if (nf > kPrMaxFrags) nf = kPrMaxFrags;   // cannot happen: fragments are non-empty
+	const uint32_t vbase = __ldg(a.pos + eb);
+	// nf <= kPrMaxFrags: every fragment of an entry inside the block has a
+	// slot in the block, and only the two end entries add others
+	uint32_t carry = 0;
+	for (uint32_t c0 = 0; c0 < nf; c0 += kPrThreads) {
+		const uint32_t i = c0 + tid;
+		uint32_t len = 0;
+		if (i < nf) { const uint2 fr = a.in.frags[f_begin + i]; ftab[i] = fr; len = frag_len(fr); }
+		// block exclusive scan of len
+		uint32_t x = len;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+			if (lane >= (uint32_t)o) x += t;
+		}
+		if (lane == 31) wsum[wid] = x;
+		__syncthreads();
+		uint32_t before = carry;
+		for (uint32_t w2 = 0; w2 < wid; w2++) before += wsum[w2];
+		if (i < nf) fstart[i] = vbase + before + x - len;
+		uint32_t tot = 0;
+		for (uint32_t w2 = 0; w2 < kPrThreads / 32; w2++) tot += wsum[w2];
+		carry += tot;
+		__syncthreads();
+	}
+	if (tid == 0) fstart[nf] = vbase + carry;
+	__syncthreads();
+
+	// phase 1: stream the block's slots into shared memory
+	{
+		const LevelTab* lt = a.in.lt;
+		uint32_t id[kPrPerThread], dw[kPrPerThread], bit[kPrPerThread];
+		bool in[kPrPerThread];
+#pragma unroll
+		for (int u = 0; u < kPrPerThread; u++) {
+			const uint32_t s = ra + u * kPrThreads + tid;
+			in[u] = s < rb && nf > 0;
+			id[u] = 0; dw[u] = 0; bit[u] = 0;
+			if (in[u]) {
+				// last fragment whose start is <= s
+				uint32_t lo = 0, hi = nf - 1;
+				while (lo < hi) {
+					const uint32_t mid = (lo + hi + 1) >> 1;
+					if (fstart[mid] <= s) lo = mid; else hi = mid - 1;
+				}
+				const uint2 fr = ftab[lo];
+				const uint32_t idx = fr.x + (s - fstart[lo]);
+				const uint32_t lv = frag_level(fr);
+				id[u] = __ldg(lt->ids[lv] + idx);
+				dw[u] = __ldg(lt->del[lv] + (idx >> 5));
+				bit[u] = idx & 31u;
+			}
+		}
+#pragma unroll
+		for (int u = 0; u < kPrPerThread; u++) {
+			double x = 0.0;
+			if (in[u] && !((dw[u] >> bit[u]) & 1u)) x = __ldg(a.contrib + id[u]);
+			vals[u * kPrThreads + tid] = x;
+		}
+	}
+	__syncthreads();
+
+	// phase 2: per-entry sums (short entries by one thread, in slot order)
+	for (uint32_t e = eb + tid; e < ee; e += kPrThreads) {
+		const uint32_t start = __ldg(a.pos + e), end = __ldg(a.pos + e + 1);
+		const uint32_t s0 = max(start, ra), s1 = min(end, rb);
+		if (s1 > s0 + kPrLong) {
+			const uint32_t q = atomicAdd(&sh_nlong, 1u);
+			longs[q] = e;
+			continue;
+		}
 		double s = 0.0;
-		if (w.valid && !longe && span > 0) s = lane_sum(a, w.f0, w.s0 - w.start, span);
-		for (unsigned m = __ballot_sync(0xffffffffu, longe); m; m &= m - 1) {
-			const int t = __ffs(m) - 1;
-			const uint32_t f0 = __shfl_sync(0xffffffffu, w.f0, t);
-			const uint32_t off = __shfl_sync(0xffffffffu, w.s0 - w.start, t);
-			const uint32_t n = __shfl_sync(0xffffffffu, span, t);
-			const double ws = warp_sum(a, f0, off, n);
-			if ((int)lane == t) s = ws;
-		}
-		if (w.valid) {
-			const uint32_t end = __ldg(a.pos + w.e + 1);
-			if (w.start < ra) a.carry_first[r] = s;        // began before the range
-			else if (end > rb) a.carry_last[r] = s;        // runs past its end
-			else pr_finish(a, w.v, s);
-		}
+		for (uint32_t k = s0; k < s1; k++) s += vals[k - ra];
+		pr_emit(a, r, ra, rb, e, start, end, s);
+	}
+	__syncthreads();
+	// long entries: one warp each, fixed lane stride and tree order
+	for (uint32_t q = wid; q < sh_nlong; q += kPrThreads / 32) {
+		const uint32_t e = longs[q];
+		const uint32_t start = __ldg(a.pos + e), end = __ldg(a.pos + e + 1);
+		const uint32_t s0 = max(start, ra), s1 = min(end, rb);
+		double s = 0.0;
+		for (uint32_t k = s0 + lane; k < s1; k += 32) s += vals[k - ra];
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+		if (lane == 0) pr_emit(a, r, ra, rb, e, start, end, s);
 	}
 }
 
-// Vertices straddling range boundaries: the thread of boundary q handles the
-// vertex that starts in range q-1 and crosses q*kPrRange.
+// Vertices straddling block boundaries: the thread of boundary q handles the
+// vertex that starts in block q-1 and crosses q*kPrRange.
 __global__ void pr_fixup(PrArgs a) {
 	const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1;
 	if (q >= a.nranges) return;
@@ -244,13 +256,12 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 			iterations == 0 ? pr_buf : nullptr);
 	LG_CUDA(cudaGetLastError(), "pr_init");
 	s->launches++;
-	const unsigned blocks = grid_for(a.nranges, kPrWarps);
 	const unsigned fix_blocks = grid_for(a.nranges, 256);
 	for (int it = 0; it < iterations; it++) {
 		a.contrib = sc[it & 1].as<double>();
 		a.contrib_next = sc[(it + 1) & 1].as<double>();
 		a.pr_out = (it == iterations - 1) ? pr_buf : nullptr;
-		pr_pull_step<<<blocks, kPrThreads, 0, st>>>(a);
+		pr_pull_step<<<a.nranges, kPrThreads, 0, st>>>(a);
 		if (a.nranges > 1) pr_fixup<<<fix_blocks, 256, 0, st>>>(a);
 	}
 	LG_CUDA(cudaGetLastError(), "pr_pull_step");

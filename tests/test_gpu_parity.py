@@ -311,3 +311,47 @@ def test_ppr_block_all_snapshots_vs_oracle():
         finally:
             for s in snaps:
                 s.close()
+
+
+def _write_level_files(golden, tmp_path):
+    files = []
+    for l, (s, d, ds, dd, w) in enumerate(golden["levels"]):
+        p = tmp_path / f"level{l}.net"
+        with open(p, "w") as f:
+            f.write("# level %d\n" % l)
+            for a, b, c in zip(s, d, w):
+                f.write(f"{a}\t{b}\t{c}\n")
+            for a, b in zip(ds, dd):
+                f.write(f"- {a}\t{b}\n")
+        files.append(str(p))
+    return files
+
+
+@pytest.mark.parametrize("task", ["pagerank_double", "bfs_count", "sssp_weighted", "tc_u"])
+def test_cli_return_value_matches_reference(golden, tmp_path, task):
+    """`lg_benchmark -r TASK FILE...` prints the reference task's return value."""
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(lb.LIB_PATH), "lg_benchmark")
+    files = _write_level_files(golden, tmp_path)
+    L = len(files) - 1
+    V = int(golden["V"])
+    root = int(golden["roots"][0])
+    # the CLI sizes the store by the largest id in the files; isolated
+    # trailing vertices change N for PageRank, so compare only when equal
+    used = max(int(x.max()) for lv in golden["levels"] for x in lv[:4] if len(x)) + 1
+    if root >= used:
+        pytest.skip("root is an isolated trailing vertex")
+    out = subprocess.run([exe, "-r", task, "-R", str(root), "-n", str(int(golden["pr_iters"]))]
+                         + files, capture_output=True, text=True, check=True).stdout
+    ret = float(out.strip().splitlines()[-1].split(":")[1])
+    if task == "pagerank_double":
+        if used != V:
+            pytest.skip("largest vertex id is isolated")
+        assert abs(ret - float(np.sum(golden[f"pr{L}"]))) <= 1e-9
+    elif task == "bfs_count":
+        assert ret == golden[f"bfscount{L}"][0]
+    elif task == "sssp_weighted":
+        assert ret == np.sum(golden[f"sssp{L}"][0] < lb._lib.LG_UNREACHED)
+    else:
+        assert ret == golden[f"tc{L}"]
