@@ -152,6 +152,7 @@ struct DevBuf {
 struct DevLevel {
 	uint64_t max_nodes = 0;
 	uint64_t n_slots = 0;
+	uint64_t n_fragment_slots = 0;   // slots that belong to this level's fragments
 	DevBuf vt;        // lg_vt_entry[max_nodes + 1]
 	DevBuf ids;       // u32[n_slots]
 	DevBuf w;         // u32[n_slots] or empty

@@ -234,8 +234,9 @@ static lg_status ingest_csr(lg_store* s, DevCsr& csr, int l,
 	// of this level.
 	std::vector<uint8_t> mask(S, 0);
 	int bad = 0;
+	uint64_t frag_slots = 0;
 	const auto& lv = csr.levels;
-#pragma omp parallel for schedule(dynamic, 65536) reduction(|:bad)
+#pragma omp parallel for schedule(dynamic, 65536) reduction(|:bad) reduction(+:frag_slots)
 	for (uint64_t v = 0; v < V; v++) {
 		const lg_vt_entry& e = vt_at(c, v);
 		if (e.adj_list_start == LG_NIL_EDGE || e.level_length == 0) continue;
@@ -245,8 +246,10 @@ static lg_status ingest_csr(lg_store* s, DevCsr& csr, int l,
 		if ((int)el > l) { bad |= 1; continue; }
 		uint64_t lim = (int)el == l ? S : lv[el]->n_slots;
 		if (ix + e.level_length > lim) { bad |= 2; continue; }
-		if ((int)el == l)
+		if ((int)el == l) {
 			for (uint64_t k = 0; k < e.level_length; k++) mask[ix + k] = 1;
+			frag_slots += e.level_length;
+		}
 	}
 	if (bad & 4) return set_error(LG_ENOTSUP, "%s: fragment longer than %u slots", name, LG_MAX_FRAGMENT_LEN);
 	if (bad & 1) return set_error(LG_EINVAL, "%s: vertex table points to a future level", name);
@@ -256,6 +259,7 @@ static lg_status ingest_csr(lg_store* s, DevCsr& csr, int l,
 	if (!d) return set_error(LG_ENOMEM, "host allocation");
 	d->max_nodes = V;
 	d->n_slots = S;
+	d->n_fragment_slots = frag_slots;
 	lg_status st = d->vt.reserve((V + 1) * sizeof(lg_vt_entry));
 	if (!st) st = d->ids.reserve(std::max<uint64_t>(S, 1) * sizeof(uint32_t));
 	if (!st && c.weights) st = d->w.reserve(std::max<uint64_t>(S, 1) * sizeof(uint32_t));
