@@ -232,6 +232,27 @@ lg_status lg_snapshot_adjacency(lg_snapshot* snap, int dir, uint64_t* offsets,
 lg_status lg_pagerank_pull(lg_snapshot* snap, int iterations, double damping,
 		double* ranks);
 
+/* The same PageRank for callers that cannot let the library allocate device
+ * memory (this entry point has no counterpart in the reference).
+ * lg_pagerank_pull grows store-owned scratch with cudaMalloc; a thread that is
+ * capturing its stream into a CUDA graph may not call cudaMalloc/cudaFree, and
+ * a process whose device memory is already handed to another allocator may see
+ * cudaMalloc fail or stall.  This variant allocates nothing: its per-iteration
+ * vectors live in a fixed LG_NOALLOC_SCRATCH_BYTES area compiled into the
+ * library, which every GPU that loads the library keeps reserved until the
+ * process exits.  The graph must fit: 24 bytes per vertex plus 16 bytes per
+ * 2048 in-CSR slots <= LG_NOALLOC_SCRATCH_BYTES (about 2.7 million vertices),
+ * otherwise LG_EINVAL.  The first call on each device looks up the area's
+ * device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture.  All calls share the one area and
+ * leave their values in it; two calls that overlap on the GPU (different
+ * streams or stores on the same device) race and must be serialised by the
+ * caller.  Same arguments and results as lg_pagerank_pull. */
+#define LG_NOALLOC_SCRATCH_BYTES (64ull << 20)
+#define LG_NOALLOC_MAX_DEVICES   64
+lg_status lg_pagerank_pull_noalloc(lg_snapshot* snap, int iterations,
+		double damping, double* ranks);
+
 /* BFS levels from `root`: u_sssp_bfs / ll_b_sssp_unweighted_bfs
  * (benchmark/benchmarks/sssp.h:219-300) over ll_bfs_template
  * (llama/include/llama/ll_bfs_template.h:152-293).  levels: int32[max_nodes],

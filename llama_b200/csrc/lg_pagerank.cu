@@ -28,6 +28,8 @@
 #include "lg_device.cuh"
 #include "lg_expand.cuh"
 
+#include <mutex>
+
 namespace lg {
 
 constexpr int kPrThreads = 256;
@@ -269,6 +271,102 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 	if (!dev_out) {
 		LG_TRY(copy_out(s, ranks, pr_buf, V * sizeof(double)));
 		LG_CUDA(cudaStreamSynchronize(st), "pagerank");
+	}
+	return LG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// PageRank without device allocation.
+//
+// lg_pagerank_pull keeps its per-iteration vectors in store-owned scratch
+// that it grows with cudaMalloc.  Some callers cannot have the library
+// allocate: a thread that is capturing work into a CUDA graph (cudaMalloc
+// and cudaFree are not allowed while its stream is being captured), or a
+// process whose device memory is already handed out to another allocator,
+// where a new cudaMalloc can fail or stall on a device-wide synchronisation.
+// For them this variant runs the same kernels on a fixed scratch area that
+// is part of the library image: LG_NOALLOC_SCRATCH_BYTES of device memory,
+// reserved on every GPU that loads the library, until the process exits.
+// ---------------------------------------------------------------------------
+
+namespace lg {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[LG_NOALLOC_SCRATCH_BYTES];
+
+} // namespace lg
+
+extern "C" lg_status lg_pagerank_pull_noalloc(lg_snapshot* sn, int iterations,
+		double damping, double* ranks) {
+	clear_error();
+	if (!sn || !ranks) return set_error(LG_EINVAL, "null argument");
+	if (!(damping > 0.0 && damping < 1.0))
+		return set_error(LG_EINVAL, "damping must be in (0, 1)");
+	if (iterations < 0) return set_error(LG_EINVAL, "iterations must be >= 0");
+	if (!sn->in.present)
+		return set_error(LG_ESTATE, "pull PageRank needs the in-CSR (reverse edges)");
+	lg_store* s = sn->store;
+	const uint64_t V = sn->V;
+	const uint64_t total = sn->in.n_frag_slots;
+	const uint64_t nranges = std::max<uint64_t>(1, (total + kPrRange - 1) / kPrRange);
+	// contrib (two vectors), the result staged for host outputs, carries
+	const uint64_t need = 3 * V * sizeof(double) + 2 * nranges * sizeof(double);
+	if (need > LG_NOALLOC_SCRATCH_BYTES)
+		return set_error(LG_EINVAL, "graph needs %llu scratch bytes, more than the %llu "
+				"this entry point has (24 B per vertex + 16 B per %u in-CSR slots)",
+				(unsigned long long)need, (unsigned long long)LG_NOALLOC_SCRATCH_BYTES,
+				kPrRange);
+	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+	// Device address of the scratch array, looked up once per device with
+	// that device current (host code must not use the symbol itself).
+	static std::mutex mu;
+	static void* scratch_of[LG_NOALLOC_MAX_DEVICES] = {};
+	if (s->device < 0 || s->device >= LG_NOALLOC_MAX_DEVICES)
+		return set_error(LG_ENOTSUP, "device ordinal %d beyond %d", s->device,
+				LG_NOALLOC_MAX_DEVICES);
+	void* base = nullptr;
+	{
+		std::lock_guard<std::mutex> lk(mu);
+		if (!scratch_of[s->device]) {
+			void* p = nullptr;
+			LG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+			scratch_of[s->device] = p;
+		}
+		base = scratch_of[s->device];
+	}
+	cudaStream_t st = s->stream;
+	double* c0 = (double*)base;
+	double* c1 = c0 + V;
+	double* staged = c1 + V;
+	double* carries = staged + V;
+
+	PrArgs a;
+	a.in = sn->view(1);
+	a.pos = sn->in.slot_off.as<uint32_t>();
+	a.total = (uint32_t)total;
+	a.nranges = (uint32_t)nranges;
+	a.outdeg = sn->out.deg.as<uint32_t>();
+	a.base = (1.0 - damping) / (double)V;
+	a.d = damping;
+	a.carry_first = carries;
+	a.carry_last = carries + nranges;
+	const bool dev_out = is_device_pointer(ranks);
+	double* pr_buf = dev_out ? ranks : staged;
+	pr_init<<<grid_for(V, 256), 256, 0, st>>>(a.outdeg, V, 1.0 / (double)V, c0,
+			iterations == 0 ? pr_buf : nullptr);
+	for (int it = 0; it < iterations; it++) {
+		a.contrib = (it & 1) ? c1 : c0;
+		a.contrib_next = (it & 1) ? c0 : c1;
+		a.pr_out = (it == iterations - 1) ? pr_buf : nullptr;
+		pr_pull_step<<<a.nranges, kPrThreads, 0, st>>>(a);
+		if (a.nranges > 1) pr_fixup<<<grid_for(a.nranges, 256), 256, 0, st>>>(a);
+	}
+	LG_CUDA(cudaGetLastError(), "pagerank noalloc");
+	s->launches += 1 + (uint64_t)iterations * (a.nranges > 1 ? 2 : 1);
+	if (!dev_out) {
+		LG_CUDA(cudaMemcpyAsync(ranks, pr_buf, V * sizeof(double), cudaMemcpyDeviceToHost, st),
+				"copy result");
+		s->d2h_bytes += V * sizeof(double);
+		LG_CUDA(cudaStreamSynchronize(st), "pagerank noalloc");
 	}
 	return LG_OK;
 }
