@@ -48,6 +48,11 @@ def parse():
     p.add_argument("--roots", type=int, default=16)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the secondary kernels (SSSP, TC, SCC, BC, PPR, adjoint)")
+    p.add_argument("--kron-scale", type=int, default=21)
+    p.add_argument("--bc-sources", type=int, default=256)
+    p.add_argument("--adjoint-scale", type=int, default=20)
     p.add_argument("--out", default=None, help="also write the JSON line here")
     return p.parse_args()
 
@@ -55,7 +60,7 @@ def parse():
 def workload(args):
     from llama_b200 import workloads
     spec = workloads.rmat_multiversion(scale=args.scale, seed=2, levels=args.levels,
-                                       level0=0.90, delete=0.002)
+                                       level0=0.90, delete=0.002, weight_max=255)
     cfg = {"workload": f"rmat{args.scale}_{args.levels}level_del0.2pct",
            "graph": f"directed R-MAT scale {args.scale}, edge factor 16, "
                     f"{args.levels} levels (90% in level 0, 0.2% deletions per level)",
@@ -328,6 +333,10 @@ def run_lg(args):
                            "PageRank + BFS with results copied to pinned host memory"}
         sn = None
 
+    ext = None
+    if not args.no_extras:
+        ext = extras(args, st, stream, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(hg, spec, roots, args)
@@ -348,7 +357,7 @@ def run_lg(args):
                       "in_fragments": ins["fragments"], "levels": hg.num_levels,
                       "host_build_s": build_s, "ingest_s": ingest_s},
             "roofline": roofline, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "cpu_baseline": cpu}
+            "clocks": clk, "cpu_baseline": cpu, "extras": ext}
     if rank == 0:
         emit(line, args)
     if sn is not None:
@@ -357,6 +366,134 @@ def run_lg(args):
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def _timed(stream, fn):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r = fn()
+    e1.record(stream)
+    stream.synchronize()
+    return r, e0.elapsed_time(e1)
+
+
+def extras(args, st, stream, device):
+    """Secondary kernels, each timed once with CUDA events on the store's
+    stream after a warm-up call: SSSP / triangle counting / SCC on the main
+    store; batched vs plain BC and the PPR block on a symmetric Kronecker
+    store; adjoint vs forward PageRank on a weighted R-MAT."""
+    import torch
+    import numpy as np
+    from llama_b200 import HostGraph, Store, workloads
+    from llama_b200.graph import ppr
+    out = {}
+    dev = f"cuda:{device}"
+
+    def guard(name, fn):
+        try:
+            out[name] = fn()
+        except Exception as e:      # a failing extra is reported, not fatal
+            out[name] = {"error": str(e)[:300]}
+
+    def on_main():
+        sn = st.snapshot()
+        try:
+            V, E = sn.max_nodes, sn.num_edges
+            res = {}
+            roots = workloads.pick_roots(sn.out_degrees(), 8, seed=13)
+            dist = torch.empty(V, dtype=torch.int32, device=dev)
+            sn.sssp(int(roots[0]), 32, out=dist)
+            reach, ms = 0, 0.0
+            for r in roots:
+                (_, rr), t = _timed(stream, lambda: sn.sssp(int(r), 32, out=dist))
+                reach += rr.reach_edges
+                ms += t
+            res["sssp_delta32_8roots"] = {"ms": ms, "gteps": reach / (ms / 1e3) / 1e9}
+            sn.triangle_count()
+            tc, ms = _timed(stream, sn.triangle_count)
+            res["triangle_count"] = {"ms": ms, "triangles": tc.triangles,
+                                     "gteps": E / (ms / 1e3) / 1e9}
+            lab = torch.empty(V, dtype=torch.int64, device=dev)
+            sn.scc(out=lab)
+            (_, sr), ms = _timed(stream, lambda: sn.scc(out=lab))
+            res["scc"] = {"ms": ms, "components": sr.components, "gteps": E / (ms / 1e3) / 1e9}
+            return res
+        finally:
+            sn.close()
+
+    def on_kron():
+        spec = workloads.kronecker_symmetric(scale=args.kron_scale, seed=6, levels=4)
+        hg = HostGraph.from_spec(spec)
+        with Store(device=device, stream=stream.cuda_stream) as s2:
+            s2.ingest(hg)
+            snaps = [s2.snapshot(l) for l in range(4)]
+            try:
+                sn = snaps[-1]
+                V, E = sn.max_nodes, sn.num_edges
+                src = workloads.pick_roots(sn.out_degrees(), args.bc_sources, seed=14)
+                bc = torch.empty(V, dtype=torch.float64, device=dev)
+                sn.bc(src[:64], batched=True, out=bc)
+                _, tb = _timed(stream, lambda: sn.bc(src, batched=True, out=bc))
+                n_plain = min(32, len(src))
+                sn.bc(src[:2], batched=False, out=bc)
+                _, tp = _timed(stream, lambda: sn.bc(src[:n_plain], batched=False, out=bc))
+                per_b, per_p = tb / len(src), tp / n_plain
+                res = {"bc": {"graph": f"Kronecker scale {args.kron_scale}, symmetric, 4 levels",
+                              "batched_ms_per_source": per_b, "plain_ms_per_source": per_p,
+                              "batched_speedup": per_p / per_b,
+                              "batched_gteps": 2 * E * len(src) / (tb / 1e3) / 1e9,
+                              "sources_batched": len(src), "sources_plain": n_plain}}
+                seeds = workloads.pick_roots(sn.out_degrees(), 256, seed=15)
+                out_ppr = torch.empty((4, V, 256), dtype=torch.float64, device=dev)
+                ppr(snaps, seeds[:32], iterations=2, out=out_ppr[:, :, :32].contiguous())
+                _, tq = _timed(stream, lambda: ppr(snaps, seeds, iterations=20, out=out_ppr))
+                e_all = sum(s.num_edges for s in snaps)
+                res["ppr"] = {"K": 256, "iterations": 20, "snapshots": 4, "ms": tq,
+                              "gteps": 20 * e_all * 256 / (tq / 1e3) / 1e9}
+                return res
+            finally:
+                for s in snaps:
+                    s.close()
+
+    def on_adjoint():
+        spec = workloads.rmat_multiversion(scale=args.adjoint_scale, seed=4, levels=1, level0=1.0)
+        hg = HostGraph.from_spec(spec)
+        with Store(device=device, stream=stream.cuda_stream) as s3:
+            s3.ingest(hg)
+            with s3.snapshot() as sn:
+                V = sn.max_nodes
+                off, nb = sn.adjacency(0)
+                rng = np.random.default_rng(4)
+                raw = rng.uniform(0.5, 1.5, len(nb))
+                srcv = np.repeat(np.arange(V), np.diff(off.astype(np.int64)))
+                w = torch.tensor(raw / np.bincount(srcv, raw, V)[srcv], device=dev)
+                v = rng.exponential(1.0, V)
+                v = torch.tensor(v / v.sum(), device=dev)
+                u = torch.empty(V, dtype=torch.float64, device=dev)
+                sn.pagerank_fwd(w, torch.full((V,), 1.0 / V, dtype=torch.float64, device=dev),
+                                0.85, keep_tape=False, out=u)
+                x = torch.empty(V, dtype=torch.float64, device=dev)
+                (_, tape, fr), tf = _timed(stream, lambda: sn.pagerank_fwd(w, v, 0.85, out=x))
+                # L = sum over 1024 targets of (x_v - 1.2 u_v)^2, u = uniform-teleport scores
+                T = torch.tensor(rng.choice(V, 1024, replace=False), device=dev)
+                g = torch.zeros(V, dtype=torch.float64, device=dev)
+                g[T] = 2 * (x[T] - 1.2 * u[T])
+                dw = torch.empty(len(nb), dtype=torch.float64, device=dev)
+                dv = torch.empty(V, dtype=torch.float64, device=dev)
+                (_, _, br), tb = _timed(stream, lambda: tape.backward(g, dw, dv))
+                tape.close()
+                return {"graph": f"R-MAT scale {args.adjoint_scale}, FP64 weights U[0.5,1.5] "
+                                 "row-normalised, Dirichlet(1) teleport, tol 1e-12",
+                        "forward_ms": tf, "forward_iterations": fr.iterations,
+                        "backward_ms": tb, "backward_iterations": br.iterations,
+                        "backward_over_forward": tb / tf}
+
+    guard("main_store", on_main)
+    guard("kronecker", on_kron)
+    guard("adjoint", on_adjoint)
+    return out
 
 
 def cpu_baseline(hg, spec, roots, args):

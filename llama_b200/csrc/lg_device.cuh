@@ -167,8 +167,12 @@ struct DevCsr {
 	~DevCsr() { for (DevLevel* l : levels) delete l; }
 };
 
+// Slots per PageRank block; range_lb below is computed for this size.
+constexpr uint32_t kBlockSlots = 1024;
+
 struct SnapDir {
 	DevBuf frag_off, frags, deg, delbits, lt, slot_off;
+	DevBuf range_lb;               // lower_bound(slot_off, r * kBlockSlots), r = 0..nblocks
 	uint64_t n_frags = 0;
 	uint64_t n_edges = 0;          // live edges (sum of degrees)
 	uint64_t n_slots = 0;          // slots of levels 0..L

@@ -32,15 +32,17 @@
 
 namespace lg {
 
-constexpr int kPrThreads = 256;
+constexpr int kPrThreads = 128;
 constexpr int kPrPerThread = 8;
-constexpr uint32_t kPrRange = kPrThreads * kPrPerThread;        // 2048 slots
+constexpr uint32_t kPrRange = kPrThreads * kPrPerThread;        // 1024 slots
+static_assert(kPrRange == kBlockSlots, "range_lb is computed for kBlockSlots");
 constexpr uint32_t kPrMaxFrags = kPrRange + 2 * LG_MAX_LEVELS;   // fragments touching a block
 constexpr uint32_t kPrLong = 64;       // entries with more slots are reduced by a warp
 
 struct PrArgs {
 	SnapCsr in;
 	const uint32_t* pos;       // V + 1 in-CSR slot prefix
+	const uint32_t* range_lb;  // nranges + 1 block entry bounds
 	uint32_t total;            // pos[V]
 	uint32_t nranges;
 	const uint32_t* outdeg;
@@ -72,6 +74,7 @@ pr_pull_step(PrArgs a) {
 	__shared__ double vals[kPrRange];
 	__shared__ uint2 ftab[kPrMaxFrags];
 	__shared__ uint32_t fstart[kPrMaxFrags + 1];
+	__shared__ uint32_t fidx[kPrRange];
 	__shared__ uint32_t longs[kPrRange / kPrLong + 2];
 	__shared__ uint32_t sh_eb, sh_ee, sh_nlong;
 	__shared__ uint32_t wsum[kPrThreads / 32];
@@ -80,10 +83,15 @@ pr_pull_step(PrArgs a) {
 	const bool last_range = r == a.nranges - 1;
 	const uint32_t ra = r * kPrRange;
 	const uint32_t rb = last_range ? a.total : min(a.total, ra + kPrRange);
-	if (wid == 0) {
-		uint32_t eb, ee;
-		range_entries(a.pos, (uint32_t)a.in.V, ra, rb, last_range, &eb, &ee);
-		if (lane == 0) { sh_eb = eb; sh_ee = ee; sh_nlong = 0; }
+	const uint32_t V = (uint32_t)a.in.V;
+	if (tid == 0) {
+		// entries of the block: those starting in [ra, rb), plus the one
+		// straddling ra (precomputed lower bounds, see block_lower_bounds)
+		uint32_t eb = __ldg(a.range_lb + r);
+		if (eb > 0 && (eb == V || __ldg(a.pos + eb) > ra)) eb--;
+		sh_eb = eb;
+		sh_ee = last_range ? V : __ldg(a.range_lb + r + 1);
+		sh_nlong = 0;
 	}
 	__syncthreads();
 	const uint32_t eb = sh_eb, ee = sh_ee;
@@ -118,39 +126,71 @@ pr_pull_step(PrArgs a) {
 		__syncthreads();
 	}
 	if (tid == 0) fstart[nf] = vbase + carry;
+	// slot -> fragment map: each fragment marks the first block slot it
+	// covers (the last of the fragments starting at or before ra marks slot
+	// 0), then an inclusive max-scan over the block's slots spreads the marks
+	for (uint32_t k = tid; k < kPrRange; k += kPrThreads) fidx[k] = 0;
+	__syncthreads();
+	for (uint32_t i = tid; i < nf; i += kPrThreads) {
+		const uint32_t st = fstart[i];
+		if (st < rb) atomicMax(&fidx[st > ra ? st - ra : 0], i);
+	}
+	__syncthreads();
+	{
+		// thread t scans slots [8t, 8t + 8) serially, then a block scan of
+		// the thread maxima carries the mark across threads
+		uint32_t m = 0, loc[kPrPerThread];
+#pragma unroll
+		for (int u = 0; u < kPrPerThread; u++) {
+			m = max(m, fidx[tid * kPrPerThread + u]);
+			loc[u] = m;
+		}
+		uint32_t x = m;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+			if (lane >= (uint32_t)o) x = max(x, t);
+		}
+		if (lane == 31) wsum[wid] = x;
+		__syncthreads();
+		uint32_t before = __shfl_up_sync(0xffffffffu, x, 1);
+		if (lane == 0) before = 0;
+		for (uint32_t w2 = 0; w2 < wid; w2++) before = max(before, wsum[w2]);
+#pragma unroll
+		for (int u = 0; u < kPrPerThread; u++)
+			fidx[tid * kPrPerThread + u] = max(before, loc[u]);
+	}
 	__syncthreads();
 
-	// phase 1: stream the block's slots into shared memory
+	// phase 1: stream the block's slots into shared memory, slot
+	// ra + u * kPrThreads + tid for thread tid (coalesced id loads); all
+	// loads of a thread are issued before any value is used
 	{
 		const LevelTab* lt = a.in.lt;
 		uint32_t id[kPrPerThread], dw[kPrPerThread], bit[kPrPerThread];
 		bool in[kPrPerThread];
 #pragma unroll
 		for (int u = 0; u < kPrPerThread; u++) {
-			const uint32_t s = ra + u * kPrThreads + tid;
+			const uint32_t k = u * kPrThreads + tid;
+			const uint32_t s = ra + k;
 			in[u] = s < rb && nf > 0;
 			id[u] = 0; dw[u] = 0; bit[u] = 0;
 			if (in[u]) {
-				// last fragment whose start is <= s
-				uint32_t lo = 0, hi = nf - 1;
-				while (lo < hi) {
-					const uint32_t mid = (lo + hi + 1) >> 1;
-					if (fstart[mid] <= s) lo = mid; else hi = mid - 1;
-				}
-				const uint2 fr = ftab[lo];
-				const uint32_t idx = fr.x + (s - fstart[lo]);
+				const uint32_t f = fidx[k];
+				const uint2 fr = ftab[f];
+				const uint32_t idx = fr.x + (s - fstart[f]);
 				const uint32_t lv = frag_level(fr);
 				id[u] = __ldg(lt->ids[lv] + idx);
 				dw[u] = __ldg(lt->del[lv] + (idx >> 5));
 				bit[u] = idx & 31u;
 			}
 		}
+		double x[kPrPerThread];
 #pragma unroll
-		for (int u = 0; u < kPrPerThread; u++) {
-			double x = 0.0;
-			if (in[u] && !((dw[u] >> bit[u]) & 1u)) x = __ldg(a.contrib + id[u]);
-			vals[u * kPrThreads + tid] = x;
-		}
+		for (int u = 0; u < kPrPerThread; u++)
+			x[u] = (in[u] && !((dw[u] >> bit[u]) & 1u)) ? __ldg(a.contrib + id[u]) : 0.0;
+#pragma unroll
+		for (int u = 0; u < kPrPerThread; u++) vals[u * kPrThreads + tid] = x[u];
 	}
 	__syncthreads();
 
@@ -236,6 +276,7 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 	PrArgs a;
 	a.in = sn->view(1);
 	a.pos = sn->in.slot_off.as<uint32_t>();
+	a.range_lb = sn->in.range_lb.as<uint32_t>();
 	a.total = (uint32_t)sn->in.n_frag_slots;
 	a.nranges = (uint32_t)std::max<uint64_t>(1, (a.total + kPrRange - 1) / kPrRange);
 	a.outdeg = sn->out.deg.as<uint32_t>();
@@ -342,6 +383,7 @@ extern "C" lg_status lg_pagerank_pull_noalloc(lg_snapshot* sn, int iterations,
 	PrArgs a;
 	a.in = sn->view(1);
 	a.pos = sn->in.slot_off.as<uint32_t>();
+	a.range_lb = sn->in.range_lb.as<uint32_t>();
 	a.total = (uint32_t)total;
 	a.nranges = (uint32_t)nranges;
 	a.outdeg = sn->out.deg.as<uint32_t>();

@@ -397,6 +397,21 @@ __global__ void mark_deletions(const uint2* dels, uint64_t n, int L,
 	atomicOr(del_words[lv] + (d.x >> 5), 1u << (d.x & 31));
 }
 
+// lb[r] = first vertex e with pos[e] >= r * kBlockSlots (pos has V + 1
+// entries), for r = 0..nb: the entry bounds of every PageRank block.
+__global__ void block_lower_bounds(const uint32_t* pos, uint64_t V, uint64_t nb,
+		uint32_t* lb) {
+	const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (r > nb) return;
+	const uint64_t x = r * kBlockSlots;
+	uint64_t lo = 0, hi = V;                     // answer in [lo, hi]
+	while (lo < hi) {
+		const uint64_t mid = (lo + hi) >> 1;
+		if (pos[mid] < x) lo = mid + 1; else hi = mid;
+	}
+	lb[r] = (uint32_t)lo;
+}
+
 __global__ void sum_u32(const uint32_t* x, uint64_t n, unsigned long long* out) {
 	unsigned long long s = 0;
 	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -473,6 +488,14 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 	LG_TRY(d.slot_off.reserve((V + 1) * sizeof(uint32_t)));
 	LG_TRY(exclusive_scan_u32(slots.as<uint32_t>(), d.slot_off.as<uint32_t>(), V,
 			scan_tmp, st, &total_slots));
+	{
+		const uint64_t nb = std::max<uint64_t>(1, (total_slots + kBlockSlots - 1) / kBlockSlots);
+		LG_TRY(d.range_lb.reserve((nb + 1) * sizeof(uint32_t)));
+		block_lower_bounds<<<grid_for(nb + 1, B), B, 0, st>>>(d.slot_off.as<uint32_t>(), V,
+				nb, d.range_lb.as<uint32_t>());
+		LG_CUDA(cudaGetLastError(), "block_lower_bounds");
+		s->launches++;
+	}
 	DevBuf counters;
 	LG_TRY(counters.reserve(sizeof(unsigned long long)));
 	LG_CUDA(cudaMemsetAsync(counters.p, 0, sizeof(unsigned long long), st), "memset");
