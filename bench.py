@@ -13,7 +13,7 @@ value    = traversed edges per second of the device-resident step:
 e2e      = the same step through the C ABI with host buffers: every step
            re-ingests the newest level from host memory (pinned staging),
            reopens the snapshot and copies ranks and BFS levels back to host
-roofline = the PageRank iteration kernel (pr_pull_step), HBM-bound
+roofline = the PageRank iteration kernel (pr_flat_step), HBM-bound
 --impl reference times the reference's own OpenMP kernels (oracle/_ref, built
 from the reference source) on the host cores for the same step.
 
@@ -138,13 +138,17 @@ def measured_peak():
 
 
 def profiled_traffic():
-    """DRAM bytes per pr_pull_step launch from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "pr_pull_step_traffic.json")
+    """DRAM bytes per pr_flat_step launch at this workload, from the line
+    `traffic_bytes_per_launch: N` of the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "pr_flat_step_rmat24.md")
     try:
         with open(path) as f:
-            return json.load(f)
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return {"dram_bytes_per_launch_scaled": float(line.split(":")[1])}
     except (OSError, ValueError):
-        return None
+        pass
+    return None
 
 
 def run_reference(args):
@@ -275,19 +279,34 @@ def run_lg(args):
     ms_max, edges_all = reduce_max_sum(ws, ms, edges)
     value = edges_all / (ms_max / 1e3) / 1e9
 
-    # roofline of the PageRank iteration kernel (in-CSR of the snapshot)
-    pr_bytes = (ins["live_edges"] * (4 + 8) + ins["slots"] / 8 + ins["fragments"] * 12
-                + V * (8 + 8 + 4))
-    launch_s = pr_ms / 1e3 / (args.steps * args.pr_iters)
+    # roofline of the PageRank iteration kernel (pr_flat_step + its fix-up
+    # over the flat live in-edges): one iteration = the difference between a
+    # 2k- and a k-iteration call on the same stream (the per-call flattening
+    # cancels), after the timed region
+    R = int(np.count_nonzero(sn.in_degrees()))
+    pr_bytes = ins["live_edges"] * (4 + 8) + R * (4 + 4 + 8)
+    k = args.pr_iters
+    diffs = []
+    for _ in range(3):
+        _, t1 = _timed(stream, lambda: sn.pagerank_pull(k, 0.85, out=pr_dev))
+        _, t2 = _timed(stream, lambda: sn.pagerank_pull(2 * k, 0.85, out=pr_dev))
+        diffs.append((t2 - t1) / k)
+    launch_s = statistics.median(diffs) / 1e3
     peak, peak_kind = measured_peak()
     achieved = pr_bytes / launch_s / 1e9
     traffic = profiled_traffic()
-    roofline = {"bound": "hbm", "kernel": "pr_pull_step", "achieved": achieved,
+    roofline = {"bound": "hbm", "kernel": "pr_flat_step", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                                if peak_kind == "measured" else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_launch": pr_bytes,
+                "bytes_model": "12 B per live in-edge (4 B id + 8 B gathered contribution) "
+                               "+ 16 B per vertex with in-edges (row start, out-degree, "
+                               "written contribution)",
                 "launch_ms": launch_s * 1e3,
+                "launch_ms_source": "CUDA events on the store's stream: "
+                                    "(t(2k iterations) - t(k iterations)) / k, median of 3",
+                "pr_call_ms": pr_ms / args.steps,
                 "traffic": traffic["dram_bytes_per_launch_scaled"] if traffic else None}
 
     # e2e: newest level re-ingested from host, snapshot reopened, results to host

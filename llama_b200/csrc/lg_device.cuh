@@ -203,7 +203,7 @@ struct lg_store {
 	size_t pinned_bytes = 0;
 	cudaEvent_t staged[2] = {nullptr, nullptr};
 	// scratch shared by the analytics calls of this store
-	lg::DevBuf scratch[8];
+	lg::DevBuf scratch[12];
 	int open_snapshots = 0;
 	uint64_t launches = 0;      // kernels launched by this store
 	uint64_t h2d_bytes = 0;     // host -> device bytes copied by this store
