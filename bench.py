@@ -5,8 +5,9 @@ Workload (default): directed R-MAT scale 24 (2^24 vertices, 16 * 2^24 draws,
 a/b/c/d = .57/.19/.19/.05, self-loops and duplicates removed, seed 2), split
 into 8 levels: a seeded 90 % of the edges form level 0, levels 1..7 each add
 ~1.4 % and delete 0.2 % of the live edges (deletion marks in older levels).
-One step on the latest snapshot = FP64 PageRank pull, 20 iterations, d = 0.85
-+ BFS from 16 roots (seed 3, out-degree > 0).
+One step on the latest snapshot = flatten its in-CSR (lg_snapshot_flatten)
++ FP64 PageRank pull, 20 iterations, d = 0.85 + BFS from 16 roots (seed 3,
+out-degree > 0) + free the flat CSR.
 
 value    = traversed edges per second of the device-resident step:
            (20 * E_live + sum over roots of E_reach) / step time  [GTEPS]
@@ -64,8 +65,8 @@ def workload(args):
     cfg = {"workload": f"rmat{args.scale}_{args.levels}level_del0.2pct",
            "graph": f"directed R-MAT scale {args.scale}, edge factor 16, "
                     f"{args.levels} levels (90% in level 0, 0.2% deletions per level)",
-           "step": f"PageRank pull FP64 x{args.pr_iters} iterations + BFS from "
-                   f"{args.roots} roots, latest snapshot",
+           "step": f"flatten the in-CSR + PageRank pull FP64 x{args.pr_iters} iterations "
+                   f"+ BFS from {args.roots} roots, latest snapshot",
            "pr_iterations": args.pr_iters, "damping": 0.85, "bfs_roots": args.roots}
     return spec, cfg
 
@@ -239,10 +240,14 @@ def run_lg(args):
 
     pr_dev = torch.empty(V, dtype=torch.float64, device=f"cuda:{local}")
     lv_dev = torch.empty((len(roots), V), dtype=torch.int32, device=f"cuda:{local}")
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
 
     def step():
+        # the in-CSR is flattened inside every step, used by PageRank and the
+        # BFS bottom-up steps, and freed at the end of the step
         ev[0].record(stream)
+        sn.flatten(1)
+        ev[3].record(stream)
         sn.pagerank_pull(args.pr_iters, 0.85, out=pr_dev)
         ev[1].record(stream)
         reach = 0
@@ -250,6 +255,7 @@ def run_lg(args):
             _, res = sn.bfs(int(r), out=lv_dev[i])
             reach += res.reach_edges
         ev[2].record(stream)
+        sn.unflatten()
         return reach
 
     for _ in range(max(3, args.warmup)):
@@ -262,12 +268,13 @@ def run_lg(args):
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     launches0 = st.launch_count
-    pr_ms, bfs_ms, edges = 0.0, 0.0, 0
+    pr_ms, bfs_ms, flat_ms, edges = 0.0, 0.0, 0.0, 0
     t_start.record(stream)
     for _ in range(args.steps):
         reach = step()
         stream.synchronize()
         pr_ms += ev[0].elapsed_time(ev[1])
+        flat_ms += ev[0].elapsed_time(ev[3])
         bfs_ms += ev[1].elapsed_time(ev[2])
         edges += args.pr_iters * E + reach
     t_end.record(stream)
@@ -283,8 +290,14 @@ def run_lg(args):
     # over the flat live in-edges): one iteration = the difference between a
     # 2k- and a k-iteration call on the same stream (the per-call flattening
     # cancels), after the timed region
+    # algorithmic bytes per iteration as the survey of the path defines them
+    # (ids, FP64 contribution gather, deletion bits, fragment descriptors,
+    # rank/contribution read+write and degree), and the flat kernel's own
+    # model (ids + gather per edge, row start/out-degree/write per row)
+    pr_bytes = (ins["live_edges"] * (4 + 8) + ins["slots"] / 8 + ins["fragments"] * 12
+                + V * (8 + 8 + 4))
     R = int(np.count_nonzero(sn.in_degrees()))
-    pr_bytes = ins["live_edges"] * (4 + 8) + R * (4 + 4 + 8)
+    flat_bytes = ins["live_edges"] * (4 + 8) + R * (4 + 4 + 8)
     k = args.pr_iters
     diffs = []
     for _ in range(3):
@@ -300,9 +313,11 @@ def run_lg(args):
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                                if peak_kind == "measured" else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_launch": pr_bytes,
-                "bytes_model": "12 B per live in-edge (4 B id + 8 B gathered contribution) "
-                               "+ 16 B per vertex with in-edges (row start, out-degree, "
-                               "written contribution)",
+                "bytes_model": "E_live*(4+8) + slots/8 + fragments*12 + V*(8+8+4)",
+                "flat_bytes_per_launch": flat_bytes,
+                "flat_bytes_model": "12 B per live in-edge (4 B id + 8 B gathered "
+                                    "contribution) + 16 B per vertex with in-edges",
+                "frac_flat_model": flat_bytes / launch_s / 1e9 / peak,
                 "launch_ms": launch_s * 1e3,
                 "launch_ms_source": "CUDA events on the store's stream: "
                                     "(t(2k iterations) - t(k iterations)) / k, median of 3",
@@ -322,6 +337,7 @@ def run_lg(args):
             st.drop_level()
             st.ingest_level(desc)
             s2 = st.snapshot()
+            s2.flatten(1)
             s2.pagerank_pull(args.pr_iters, 0.85, out=pr_host)
             reach = 0
             for i, r in enumerate(roots):
@@ -349,7 +365,8 @@ def run_lg(args):
                "d2h_bytes_per_step": (d1 - d0) // args.steps,
                "ms_per_step": e2e_ms_max / args.steps,
                "includes": "ingest of the newest level from host + snapshot open + "
-                           "PageRank + BFS with results copied to pinned host memory"}
+                           "in-CSR flatten + PageRank + BFS with results copied to "
+                           "pinned host memory"}
         sn = None
 
     ext = None
@@ -367,7 +384,9 @@ def run_lg(args):
             "data": "synthetic (seeded R-MAT generator, no dataset)",
             "config": dict(cfg, l2="inputs larger than L2: store %.1f GB on the device"
                            % (st.device_bytes / 1e9)),
-            "kernels": {"pagerank_pull": {"ms_per_step": pr_ms / args.steps,
+            "kernels": {"flatten_in_csr": {"ms_per_step": flat_ms / args.steps},
+                        "pagerank_pull": {"ms_per_step": pr_ms / args.steps,
+                                          "includes": "the in-CSR flatten",
                                           "gteps": args.pr_iters * E * args.steps / (pr_ms / 1e3) / 1e9},
                         "bfs": {"ms_per_step": bfs_ms / args.steps,
                                 "gteps": (edges - args.pr_iters * E * args.steps)

@@ -199,7 +199,7 @@ typedef struct lg_snapshot_stats {
 	                           records included                           */
 	uint64_t fragment_slots;/* slots covered by the vertices' fragments   */
 	uint64_t fragments;     /* (vertex, level) fragments                  */
-	uint64_t ranges;        /* 2048-slot work ranges of the slot space    */
+	uint64_t ranges;        /* 1024-slot work blocks of the slot space    */
 	uint64_t deletions;     /* deletion marks visible in the snapshot     */
 } lg_snapshot_stats;
 lg_status lg_snapshot_get_stats(const lg_snapshot* snap, int dir,
@@ -219,6 +219,25 @@ lg_status lg_in_degrees(lg_snapshot* snap, uint32_t* degrees);
  * neighbors: uint32[num edges]; edge_ids: int64 edge ids (may be NULL). */
 lg_status lg_snapshot_adjacency(lg_snapshot* snap, int dir, uint64_t* offsets,
 		uint32_t* neighbors, int64_t* edge_ids);
+
+/* Flatten one direction (0 out, 1 in) of the snapshot into a single-level
+ * CSR kept on the device with the snapshot: the live adjacency in iteration
+ * order (the sequence lg_snapshot_adjacency returns), as the task "flatten"
+ * builds a one-level graph from all levels on the host
+ * (ll_t_flatten, benchmark/tools/flatten.h).  Later traversals of that
+ * direction on this snapshot (lg_pagerank_pull; lg_bfs top-down for dir 0,
+ * bottom-up for dir 1) read the flat CSR instead of walking fragments and
+ * deletion bits; results are unchanged.  Holds about 4 B per live edge plus
+ * 20 B per vertex of device memory until lg_snapshot_unflatten or
+ * lg_snapshot_close, which hand it back to the store: the store keeps up to
+ * two released flat CSRs for later flattens (freed by lg_store_destroy).
+ * A no-op if the direction is already flat.  LG_ESTATE if dir is 1 and the
+ * store keeps no in-CSR. */
+lg_status lg_snapshot_flatten(lg_snapshot* snap, int dir);
+/* Releases the flat CSRs of both directions (waits for the store's stream). */
+lg_status lg_snapshot_unflatten(lg_snapshot* snap);
+/* *flat = 1 if direction dir of the snapshot is flattened, else 0. */
+lg_status lg_snapshot_is_flat(const lg_snapshot* snap, int dir, int* flat);
 
 /* ---------------------------------------------------------------------------
  * Analytics kernels (the benchmark tasks of benchmark/benchmark.cc:871-946).

@@ -4,7 +4,7 @@ The engine is liblg.so (hand-written sm_100a CUDA behind the C ABI in
 include/lg.h); this package is its Python mirror of the reference's
 database / snapshot / benchmark-task interface.
 """
-from ._lib import LgError, lib, LIB_PATH  # noqa: F401  (raises if not built)
+from ._lib import LG_UNREACHED, LgError, lib, LIB_PATH  # noqa: F401  (raises if not built)
 from .graph import GraphSpec, HostGraph, Snapshot, Store  # noqa: F401
 from . import workloads  # noqa: F401
 

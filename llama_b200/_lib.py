@@ -136,6 +136,9 @@ SIGNATURES = [
     ("lg_out_degrees", _INT, [_P, _P]),
     ("lg_in_degrees", _INT, [_P, _P]),
     ("lg_snapshot_adjacency", _INT, [_P, _INT, _P, _P, _P]),
+    ("lg_snapshot_flatten", _INT, [_P, _INT]),
+    ("lg_snapshot_unflatten", _INT, [_P]),
+    ("lg_snapshot_is_flat", _INT, [_P, _INT, C.POINTER(_INT)]),
     ("lg_pagerank_pull", _INT, [_P, _INT, _D, _P]),
     ("lg_pagerank_pull_noalloc", _INT, [_P, _INT, _D, _P]),
     ("lg_bfs", _INT, [_P, _I64, _P, C.POINTER(lg_bfs_result)]),

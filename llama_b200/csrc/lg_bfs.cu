@@ -9,14 +9,16 @@
 // frontier queue over the out-CSR with warp_expand, bottom-up steps let every
 // unvisited vertex look for a parent among its in-neighbours (in-CSR) in a
 // frontier bitmap that stays resident in L2.
-#include "lg_device.cuh"
 #include "lg_expand.cuh"
+#include "lg_flat.cuh"
 
 namespace lg {
 
 constexpr int32_t kUnreached = LG_UNREACHED;
 constexpr int kBfsThreads = 256;
 constexpr uint32_t kBfsRange = 1024;
+constexpr int kBuChunk = 4;            // in-neighbours a bottom-up round checks
+constexpr int kBuVerts = 4;            // vertices a flat bottom-up thread interleaves
 
 __global__ void bfs_init(int32_t* level, uint64_t V, uint32_t root,
 		uint32_t* queue, const uint32_t* outdeg, unsigned long long* ctr) {
@@ -129,10 +131,21 @@ bfs_bottom_up(SnapCsr in, const uint32_t* outdeg, const uint32_t* bits,
 			const uint2 fr = in.frags[f];
 			const uint32_t lv = frag_level(fr), n = frag_len(fr);
 			const uint32_t* ids = in.lt->ids[lv] + fr.x;
-			for (uint32_t k = 0; k < n; k++) {
-				uint32_t u = __ldg(ids + k);
-				if ((__ldg(bits + (u >> 5)) >> (u & 31)) & 1u) {
-					if (!slot_deleted(in.lt, lv, fr.x + k)) { found = true; break; }
+			// kBuChunk neighbours per round: their id and bitmap loads are
+			// independent, so a round costs two memory latencies, not 2 x kBuChunk
+			for (uint32_t k = 0; k < n && !found; k += kBuChunk) {
+				uint32_t u[kBuChunk], w[kBuChunk];
+#pragma unroll
+				for (int j = 0; j < kBuChunk; j++)
+					u[j] = k + j < n ? __ldg(ids + k + j) : kNoId;
+#pragma unroll
+				for (int j = 0; j < kBuChunk; j++)
+					w[j] = u[j] != kNoId ? __ldg(bits + (u[j] >> 5)) : 0u;
+#pragma unroll
+				for (int j = 0; j < kBuChunk; j++) {
+					if (!found && ((w[j] >> (u[j] & 31u)) & 1u)
+							&& !slot_deleted(in.lt, lv, fr.x + k + j))
+						found = true;
 				}
 			}
 		}
@@ -140,6 +153,58 @@ bfs_bottom_up(SnapCsr in, const uint32_t* outdeg, const uint32_t* bits,
 	}
 	warp_append(found, v, next, ctr);
 	warp_add_u64(found ? __ldg(outdeg + v) : 0ull, ctr + 1);
+}
+
+// Bottom-up step over a flat in-CSR (lg_snapshot_flatten).  A thread takes
+// kBuVerts vertices (kBfsThreads apart, so the level and offset loads stay
+// coalesced) and checks kBuChunk in-neighbours of each of them per round:
+// up to kBuVerts x kBuChunk id loads, then as many bitmap loads, in flight
+// at once.  No deletion bits: the flat CSR holds live edges only.
+__global__ void __launch_bounds__(kBfsThreads)
+bfs_bottom_up_flat(const uint32_t* off, const uint32_t* ids, uint32_t V,
+		const uint32_t* outdeg, const uint32_t* bits, int32_t* level,
+		uint32_t* next, unsigned long long* ctr, int32_t cur) {
+	const uint32_t base = blockIdx.x * (uint32_t)(kBfsThreads * kBuVerts) + threadIdx.x;
+	uint32_t k[kBuVerts], end[kBuVerts];
+	bool found[kBuVerts];
+#pragma unroll
+	for (int j = 0; j < kBuVerts; j++) {
+		const uint32_t v = base + j * kBfsThreads;
+		k[j] = 0; end[j] = 0; found[j] = false;
+		if (v < V && level[v] == kUnreached) { k[j] = __ldg(off + v); end[j] = __ldg(off + v + 1); }
+	}
+	bool more = true;
+	while (more) {
+		uint32_t u[kBuVerts][kBuChunk], w[kBuVerts][kBuChunk];
+#pragma unroll
+		for (int j = 0; j < kBuVerts; j++)
+#pragma unroll
+			for (int c = 0; c < kBuChunk; c++)
+				u[j][c] = k[j] + c < end[j] ? __ldg(ids + k[j] + c) : kNoId;
+#pragma unroll
+		for (int j = 0; j < kBuVerts; j++)
+#pragma unroll
+			for (int c = 0; c < kBuChunk; c++)
+				w[j][c] = u[j][c] != kNoId ? __ldg(bits + (u[j][c] >> 5)) : 0u;
+		more = false;
+#pragma unroll
+		for (int j = 0; j < kBuVerts; j++) {
+			bool hit = false;
+#pragma unroll
+			for (int c = 0; c < kBuChunk; c++) hit |= ((w[j][c] >> (u[j][c] & 31u)) & 1u) != 0;
+			if (hit) { found[j] = true; k[j] = end[j]; }
+			else k[j] = min(k[j] + kBuChunk, end[j]);
+			more |= k[j] < end[j];
+		}
+	}
+	unsigned long long mf = 0;
+#pragma unroll
+	for (int j = 0; j < kBuVerts; j++) {
+		const uint32_t v = base + j * kBfsThreads;
+		if (found[j]) { level[v] = cur + 1; mf += __ldg(outdeg + v); }
+		warp_append(found[j], v, next, ctr);
+	}
+	warp_add_u64(mf, ctr + 1);
 }
 
 } // namespace lg
@@ -175,7 +240,10 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 	uint32_t* nq = sc[1].as<uint32_t>();
 	uint32_t* bits = sc[2].as<uint32_t>();
 	unsigned long long* ctr = sc[3].as<unsigned long long>();
-	const SnapCsr out = sn->view(0);
+	// flat views where lg_snapshot_flatten made them
+	const FlatCsr* fo = sn->flat[0];
+	const FlatCsr* fi = sn->flat[1];
+	const SnapCsr out = (fo && fo->has_view) ? fo->view(sn->out.deg.as<uint32_t>()) : sn->view(0);
 	const SnapCsr in = sn->in.present ? sn->view(1) : out;
 	const uint32_t* outdeg = sn->out.deg.as<uint32_t>();
 
@@ -215,8 +283,13 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 		} else {
 			LG_CUDA(cudaMemsetAsync(bits, 0, ((V + 31) / 32) * 4, st), "memset");
 			bfs_set_bits<<<grid_for(qlen, 256), 256, 0, st>>>(q, (uint32_t)qlen, bits);
-			bfs_bottom_up<<<grid_for(V, kBfsThreads), kBfsThreads, 0, st>>>(
-					in, outdeg, bits, lvl, nq, ctr, cur);
+			if (fi)
+				bfs_bottom_up_flat<<<grid_for(V, kBfsThreads * kBuVerts), kBfsThreads, 0, st>>>(
+						fi->off.as<uint32_t>(), fi->ids.as<uint32_t>(), (uint32_t)V, outdeg,
+						bits, lvl, nq, ctr, cur);
+			else
+				bfs_bottom_up<<<grid_for(V, kBfsThreads), kBfsThreads, 0, st>>>(
+						in, outdeg, bits, lvl, nq, ctr, cur);
 			bu_steps++;
 			s->launches += 2;
 		}

@@ -190,6 +190,8 @@ struct SnapDir {
 	}
 };
 
+struct FlatCsr;   // lg_flat.cuh
+
 } // namespace lg
 
 struct lg_store {
@@ -208,6 +210,8 @@ struct lg_store {
 	uint64_t launches = 0;      // kernels launched by this store
 	uint64_t h2d_bytes = 0;     // host -> device bytes copied by this store
 	uint64_t d2h_bytes = 0;     // device -> host bytes copied by this store
+	lg::FlatCsr* flat_scratch = nullptr;   // per-call flat in-CSR of PageRank
+	lg::FlatCsr* flat_spare[2] = {nullptr, nullptr};   // unflattened, kept for reuse
 };
 
 // Edge-order maps of a snapshot used by the differentiable PageRank
@@ -218,6 +222,7 @@ void lg_free_adjoint_maps(lg_adjoint_maps* m);
 struct lg_snapshot {
 	lg_store* store = nullptr;
 	lg_adjoint_maps* adj_maps = nullptr;
+	lg::FlatCsr* flat[2] = {nullptr, nullptr};   // lg_snapshot_flatten, per direction
 	int level = 0;
 	uint64_t V = 0;
 	lg::SnapDir out, in;

@@ -13,16 +13,11 @@
 // added differs from the reference's left-to-right loop (FP64, well within
 // 1e-12 in every case), and it is fixed, so results are deterministic.
 //
-// lg_pagerank_pull first flattens the snapshot's live in-adjacency once per
-// call (flat_count / flat_write: the virtual slot space of the in-CSR in
-// vertex order, each vertex's fragments newest first, deleted slots
-// dropped), then runs every iteration over that flat edge array:
-//
-//   flat ids    E x u32      in-neighbour of every live in-edge
-//   heads       bit per edge set where a vertex's in-edges begin
-//   nz_rows     R x u32      the vertices with in-edges, in order
-//   nz_off      R x u32      where each of them begins in the flat array
-//   tile_seg    per tile     heads before the tile's first edge
+// lg_pagerank_pull runs every iteration over the snapshot's live
+// in-adjacency flattened into one CSR (lg_flat.cuh: ids in iteration order,
+// head bits where a vertex's in-edges begin, the rows with in-edges): the
+// snapshot's own when lg_snapshot_flatten made one, else one built for the
+// call in store scratch.
 //
 // pr_flat_step gives each warp a tile of kFlatTile consecutive edges, 8 per
 // lane: it issues the tile's id loads and gathers up front, adds each
@@ -36,266 +31,14 @@
 // lg_pagerank_pull_noalloc cannot hold the E-sized flat array, so it walks
 // the fragments directly every iteration (pr_pull_step, one CTA per 1024
 // virtual slots, values staged in shared memory).
-#include "lg_device.cuh"
-#include "lg_expand.cuh"
+#include "lg_flat.cuh"
 
 #include <mutex>
 
 namespace lg {
 
-constexpr int kPrThreads = 128;
-constexpr int kPrPerThread = 8;
-constexpr uint32_t kPrRange = kPrThreads * kPrPerThread;        // 1024 slots
-static_assert(kPrRange == kBlockSlots, "range_lb is computed for kBlockSlots");
-constexpr uint32_t kPrMaxFrags = kPrRange + 2 * LG_MAX_LEVELS;   // fragments touching a block
 constexpr uint32_t kPrLong = 64;       // entries with more slots are reduced by a warp
-
-// The in-CSR virtual slot space of a snapshot cut into kPrRange-slot blocks.
-struct SlotSpace {
-	SnapCsr in;
-	const uint32_t* pos;       // V + 1 in-CSR slot prefix
-	const uint32_t* range_lb;  // nranges + 1 block entry bounds
-	uint32_t total;            // pos[V]
-	uint32_t nranges;
-};
-
-// Shared-memory map from the slots of one block to their fragments.
-struct BlockMap {
-	uint2 ftab[kPrMaxFrags];           // fragments of the block's entries
-	uint32_t fstart[kPrMaxFrags + 1];  // their absolute virtual starts
-	uint32_t fidx[kPrRange];           // block slot -> index into ftab
-	uint32_t wsum[kPrThreads / 32];
-	uint32_t eb, ee, nf;               // block entries [eb, ee), fragments
-};
-
-// Builds m for block r (slots [ra, rb)); every thread of the block calls it
-// and it returns synchronised.
-__device__ void map_block(const SlotSpace& sp, uint32_t r, uint32_t ra, uint32_t rb,
-		BlockMap& m) {
-	const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
-	const bool last_range = r == sp.nranges - 1;
-	const uint32_t V = (uint32_t)sp.in.V;
-	if (tid == 0) {
-		// entries of the block: those starting in [ra, rb), plus the one
-		// straddling ra (precomputed lower bounds, see block_lower_bounds)
-		uint32_t eb = __ldg(sp.range_lb + r);
-		if (eb > 0 && (eb == V || __ldg(sp.pos + eb) > ra)) eb--;
-		m.eb = eb;
-		m.ee = last_range ? V : __ldg(sp.range_lb + r + 1);
-	}
-	__syncthreads();
-	const uint32_t eb = m.eb, ee = m.ee;
-
-	// fragment table of the block's entries, with absolute virtual starts
-	const uint32_t f_begin = __ldg(sp.in.frag_off + eb);
-	uint32_t nf = (ee > eb) ? __ldg(sp.in.frag_off + ee) - f_begin : 0;
-	// every fragment of an entry inside the block has a slot in the block,
-	// and only the two end entries add others, so nf <= kPrMaxFrags
-	if (nf > kPrMaxFrags) nf = kPrMaxFrags;
-	const uint32_t vbase = __ldg(sp.pos + eb);
-	uint32_t carry = 0;
-	for (uint32_t c0 = 0; c0 < nf; c0 += kPrThreads) {
-		const uint32_t i = c0 + tid;
-		uint32_t len = 0;
-		if (i < nf) { const uint2 fr = sp.in.frags[f_begin + i]; m.ftab[i] = fr; len = frag_len(fr); }
-		// block exclusive scan of len
-		uint32_t x = len;
-#pragma unroll
-		for (int o = 1; o < 32; o <<= 1) {
-			const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
-			if (lane >= (uint32_t)o) x += t;
-		}
-		if (lane == 31) m.wsum[wid] = x;
-		__syncthreads();
-		uint32_t before = carry;
-		for (uint32_t w2 = 0; w2 < wid; w2++) before += m.wsum[w2];
-		if (i < nf) m.fstart[i] = vbase + before + x - len;
-		uint32_t tot = 0;
-		for (uint32_t w2 = 0; w2 < kPrThreads / 32; w2++) tot += m.wsum[w2];
-		carry += tot;
-		__syncthreads();
-	}
-	if (tid == 0) { m.fstart[nf] = vbase + carry; m.nf = nf; }
-	// slot -> fragment map: each fragment marks the first block slot it
-	// covers (the last of the fragments starting at or before ra marks slot
-	// 0), then an inclusive max-scan over the block's slots spreads the marks
-	for (uint32_t k = tid; k < kPrRange; k += kPrThreads) m.fidx[k] = 0;
-	__syncthreads();
-	for (uint32_t i = tid; i < nf; i += kPrThreads) {
-		const uint32_t st = m.fstart[i];
-		if (st < rb) atomicMax(&m.fidx[st > ra ? st - ra : 0], i);
-	}
-	__syncthreads();
-	{
-		// thread t scans slots [8t, 8t + 8) serially, then a block scan of
-		// the thread maxima carries the mark across threads
-		uint32_t mx = 0, loc[kPrPerThread];
-#pragma unroll
-		for (int u = 0; u < kPrPerThread; u++) {
-			mx = max(mx, m.fidx[tid * kPrPerThread + u]);
-			loc[u] = mx;
-		}
-		uint32_t x = mx;
-#pragma unroll
-		for (int o = 1; o < 32; o <<= 1) {
-			const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
-			if (lane >= (uint32_t)o) x = max(x, t);
-		}
-		if (lane == 31) m.wsum[wid] = x;
-		__syncthreads();
-		uint32_t before = __shfl_up_sync(0xffffffffu, x, 1);
-		if (lane == 0) before = 0;
-		for (uint32_t w2 = 0; w2 < wid; w2++) before = max(before, m.wsum[w2]);
-#pragma unroll
-		for (int u = 0; u < kPrPerThread; u++)
-			m.fidx[tid * kPrPerThread + u] = max(before, loc[u]);
-	}
-	__syncthreads();
-}
-
-// Level and in-level index of block slot k (virtual slot ra + k); false if
-// the block has no such slot.
-__device__ __forceinline__ bool block_slot(const BlockMap& m, uint32_t ra, uint32_t rb,
-		uint32_t k, uint32_t* lv, uint32_t* idx) {
-	const uint32_t s = ra + k;
-	if (s >= rb || m.nf == 0) return false;
-	const uint32_t f = m.fidx[k];
-	const uint2 fr = m.ftab[f];
-	*idx = fr.x + (s - m.fstart[f]);
-	*lv = frag_level(fr);
-	return true;
-}
-
-__device__ __forceinline__ uint32_t block_end(const SlotSpace& sp, uint32_t r) {
-	const uint32_t ra = r * kPrRange;
-	return r == sp.nranges - 1 ? sp.total : min(sp.total, ra + kPrRange);
-}
-
-// ---------------------------------------------------------------------------
-// Flattening the live in-adjacency
-// ---------------------------------------------------------------------------
-
-// blk_live[r] = live slots of block r.
-__global__ void __launch_bounds__(kPrThreads)
-flat_count(SlotSpace sp, uint32_t* blk_live) {
-	__shared__ BlockMap m;
-	__shared__ uint32_t red[kPrThreads / 32];
-	const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
-	const uint32_t r = blockIdx.x, ra = r * kPrRange, rb = block_end(sp, r);
-	map_block(sp, r, ra, rb, m);
-	uint32_t c = 0;
-#pragma unroll
-	for (int u = 0; u < kPrPerThread; u++) {
-		uint32_t lv, idx;
-		if (block_slot(m, ra, rb, u * kPrThreads + tid, &lv, &idx))
-			c += !slot_deleted(sp.in.lt, lv, idx);
-	}
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-	if (lane == 0) red[wid] = c;
-	__syncthreads();
-	if (tid == 0) {
-		uint32_t t = 0;
-		for (int w = 0; w < kPrThreads / 32; w++) t += red[w];
-		blk_live[r] = t;
-	}
-}
-
-// Writes the live slots of block r to flat_ids[blk_base[r] ...] in slot
-// order, and flat_off[e] for every entry e that starts in the block
-// (flat_off has V + 1 entries; the last block also writes the trailing ones).
-__global__ void __launch_bounds__(kPrThreads)
-flat_write(SlotSpace sp, const uint32_t* blk_base, uint32_t* flat_ids, uint32_t* flat_off) {
-	constexpr int kGroups = kPrPerThread * (kPrThreads / 32);
-	__shared__ BlockMap m;
-	__shared__ uint16_t rank[kPrRange];
-	__shared__ uint32_t gpre[kGroups];
-	const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
-	const uint32_t r = blockIdx.x, ra = r * kPrRange, rb = block_end(sp, r);
-	map_block(sp, r, ra, rb, m);
-	uint32_t id[kPrPerThread], mask[kPrPerThread];
-#pragma unroll
-	for (int u = 0; u < kPrPerThread; u++) {
-		uint32_t lv = 0, idx = 0;
-		bool live = block_slot(m, ra, rb, u * kPrThreads + tid, &lv, &idx);
-		if (live) live = !slot_deleted(sp.in.lt, lv, idx);
-		id[u] = live ? __ldg(sp.in.lt->ids[lv] + idx) : 0u;
-		mask[u] = __ballot_sync(0xffffffffu, live);
-	}
-	// slot order is k = u * kPrThreads + wid * 32 + lane: group u * 4 + wid
-	if (lane == 0) {
-#pragma unroll
-		for (int u = 0; u < kPrPerThread; u++) gpre[u * (kPrThreads / 32) + wid] = __popc(mask[u]);
-	}
-	__syncthreads();
-	if (wid == 0) {
-		const uint32_t c = lane < (uint32_t)kGroups ? gpre[lane] : 0u;
-		uint32_t x = c;
-#pragma unroll
-		for (int o = 1; o < 32; o <<= 1) {
-			const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
-			if (lane >= (uint32_t)o) x += t;
-		}
-		if (lane < (uint32_t)kGroups) gpre[lane] = x - c;
-	}
-	__syncthreads();
-	const uint32_t base = __ldg(blk_base + r);
-	const uint32_t below = (1u << lane) - 1u;
-#pragma unroll
-	for (int u = 0; u < kPrPerThread; u++) {
-		const uint32_t k = u * kPrThreads + tid;
-		const uint32_t rk = gpre[u * (kPrThreads / 32) + wid] + __popc(mask[u] & below);
-		rank[k] = (uint16_t)rk;
-		if ((mask[u] >> lane) & 1u) flat_ids[base + rk] = id[u];
-	}
-	__syncthreads();
-	const uint32_t V = (uint32_t)sp.in.V;
-	const bool last = r == sp.nranges - 1;
-	const uint32_t e_begin = __ldg(sp.range_lb + r);
-	const uint32_t e_end = last ? V + 1 : __ldg(sp.range_lb + r + 1);
-	const uint32_t next = __ldg(blk_base + r + 1);
-	for (uint32_t e = e_begin + tid; e < e_end; e += kPrThreads) {
-		const uint32_t p = __ldg(sp.pos + e);
-		flat_off[e] = p < rb ? base + rank[p - ra] : next;
-	}
-}
-
-__global__ void flat_flags(const uint32_t* flat_off, uint64_t V, uint32_t* flags) {
-	const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	if (v >= V) return;
-	flags[v] = __ldg(flat_off + v + 1) > __ldg(flat_off + v);
-}
-
-__global__ void flat_rows(const uint32_t* flat_off, const uint32_t* kidx, uint64_t V,
-		uint32_t* nz_rows, uint32_t* nz_off, uint32_t* heads) {
-	const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	if (v >= V) return;
-	const uint32_t o = __ldg(flat_off + v);
-	if (__ldg(flat_off + v + 1) == o) return;
-	const uint32_t k = __ldg(kidx + v);
-	nz_rows[k] = (uint32_t)v;
-	nz_off[k] = o;
-	atomicOr(heads + (o >> 5), 1u << (o & 31u));
-}
-
-constexpr int kFlatPerLane = 8;                         // consecutive edges per lane
-constexpr uint32_t kFlatTile = 32u * kFlatPerLane;      // edges per warp
-constexpr uint32_t kFlatTileWords = kFlatTile / 32u;    // head words per tile
-constexpr int kFlatWarps = 8;                           // warps per CTA
-
-// tile_seg[t] = number of rows beginning before edge t * kFlatTile.
-__global__ void flat_tiles(const uint32_t* nz_off, uint32_t R, uint32_t ntiles,
-		uint32_t* tile_seg) {
-	const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= ntiles) return;
-	const uint32_t x = t * kFlatTile;
-	uint32_t lo = 0, hi = R;
-	while (lo < hi) {
-		const uint32_t mid = (lo + hi) >> 1;
-		if (__ldg(nz_off + mid) < x) lo = mid + 1; else hi = mid;
-	}
-	tile_seg[t] = lo;
-}
+constexpr int kFlatWarps = 8;          // warps (tiles) per CTA of pr_flat_step
 
 // ---------------------------------------------------------------------------
 // Iterations over the flat array
@@ -349,10 +92,12 @@ pr_flat_step(FlatArgs a) {
 	const uint32_t hnext = __ldg(hbytes + (size_t)(t + 1) * (kFlatTile / 8)) & 1u;
 	uint32_t id[kFlatPerLane];
 	if (eb + kFlatPerLane <= a.E) {
-		const uint4 p0 = __ldcs(reinterpret_cast<const uint4*>(a.ids + eb));
-		const uint4 p1 = __ldcs(reinterpret_cast<const uint4*>(a.ids + eb) + 1);
-		id[0] = p0.x; id[1] = p0.y; id[2] = p0.z; id[3] = p0.w;
-		id[4] = p1.x; id[5] = p1.y; id[6] = p1.z; id[7] = p1.w;
+		// one 32-byte load per lane (eb is a multiple of 8), evict-first so
+		// the streamed ids do not push the gathered contributions out of L2
+		asm("ld.global.cs.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+			: "=r"(id[0]), "=r"(id[1]), "=r"(id[2]), "=r"(id[3]),
+			  "=r"(id[4]), "=r"(id[5]), "=r"(id[6]), "=r"(id[7])
+			: "l"(a.ids + eb));
 	} else {
 #pragma unroll
 		for (int i = 0; i < kFlatPerLane; i++)
@@ -510,31 +255,31 @@ __device__ __forceinline__ void pr_emit(const PrArgs& a, uint32_t r, uint32_t ra
 	else pr_finish(a, e, s);
 }
 
-// One CTA per block of kPrRange virtual slots.  Phase 1 streams the block's
-// slots (slot ra + u * kPrThreads + tid for thread tid, coalesced id loads,
+// One CTA per block of kMapRange virtual slots.  Phase 1 streams the block's
+// slots (slot ra + u * kMapThreads + tid for thread tid, coalesced id loads,
 // all loads of a thread issued before any value is used) into shared
 // memory; phase 2 sums each vertex's values (one thread per short vertex, a
 // warp per long one).  A vertex straddling blocks leaves a partial per block
 // that pr_fixup adds in block order.
-__global__ void __launch_bounds__(kPrThreads)
+__global__ void __launch_bounds__(kMapThreads)
 pr_pull_step(PrArgs a) {
 	__shared__ BlockMap m;
-	__shared__ double vals[kPrRange];
-	__shared__ uint32_t longs[kPrRange / kPrLong + 2];
+	__shared__ double vals[kMapRange];
+	__shared__ uint32_t longs[kMapRange / kPrLong + 2];
 	__shared__ uint32_t sh_nlong;
 	const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
-	const uint32_t r = blockIdx.x, ra = r * kPrRange, rb = block_end(a.sp, r);
+	const uint32_t r = blockIdx.x, ra = r * kMapRange, rb = block_end(a.sp, r);
 	if (tid == 0) sh_nlong = 0;
 	map_block(a.sp, r, ra, rb, m);
 	const uint32_t eb = m.eb, ee = m.ee;
 	{
-		const LevelTab* lt = a.sp.in.lt;
-		uint32_t id[kPrPerThread], dw[kPrPerThread], bit[kPrPerThread];
-		bool in[kPrPerThread];
+		const LevelTab* lt = a.sp.g.lt;
+		uint32_t id[kMapPerThread], dw[kMapPerThread], bit[kMapPerThread];
+		bool in[kMapPerThread];
 #pragma unroll
-		for (int u = 0; u < kPrPerThread; u++) {
+		for (int u = 0; u < kMapPerThread; u++) {
 			uint32_t lv = 0, idx = 0;
-			in[u] = block_slot(m, ra, rb, u * kPrThreads + tid, &lv, &idx);
+			in[u] = block_slot(m, ra, rb, u * kMapThreads + tid, &lv, &idx);
 			id[u] = 0; dw[u] = 0; bit[u] = 0;
 			if (in[u]) {
 				id[u] = __ldg(lt->ids[lv] + idx);
@@ -542,17 +287,17 @@ pr_pull_step(PrArgs a) {
 				bit[u] = idx & 31u;
 			}
 		}
-		double x[kPrPerThread];
+		double x[kMapPerThread];
 #pragma unroll
-		for (int u = 0; u < kPrPerThread; u++)
+		for (int u = 0; u < kMapPerThread; u++)
 			x[u] = (in[u] && !((dw[u] >> bit[u]) & 1u)) ? __ldg(a.contrib + id[u]) : 0.0;
 #pragma unroll
-		for (int u = 0; u < kPrPerThread; u++) vals[u * kPrThreads + tid] = x[u];
+		for (int u = 0; u < kMapPerThread; u++) vals[u * kMapThreads + tid] = x[u];
 	}
 	__syncthreads();
 
 	// phase 2: per-entry sums (short entries by one thread, in slot order)
-	for (uint32_t e = eb + tid; e < ee; e += kPrThreads) {
+	for (uint32_t e = eb + tid; e < ee; e += kMapThreads) {
 		const uint32_t start = __ldg(a.sp.pos + e), end = __ldg(a.sp.pos + e + 1);
 		const uint32_t s0 = max(start, ra), s1 = min(end, rb);
 		if (s1 > s0 + kPrLong) {
@@ -566,7 +311,7 @@ pr_pull_step(PrArgs a) {
 	}
 	__syncthreads();
 	// long entries: one warp each, fixed lane stride and tree order
-	for (uint32_t q = wid; q < sh_nlong; q += kPrThreads / 32) {
+	for (uint32_t q = wid; q < sh_nlong; q += kMapThreads / 32) {
 		const uint32_t e = longs[q];
 		const uint32_t start = __ldg(a.sp.pos + e), end = __ldg(a.sp.pos + e + 1);
 		const uint32_t s0 = max(start, ra), s1 = min(end, rb);
@@ -579,22 +324,22 @@ pr_pull_step(PrArgs a) {
 }
 
 // Vertices straddling block boundaries: the thread of boundary q handles the
-// vertex that starts in block q-1 and crosses q*kPrRange.
+// vertex that starts in block q-1 and crosses q*kMapRange.
 __global__ void pr_fixup(PrArgs a) {
 	const uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1;
 	if (q >= a.sp.nranges) return;
-	const uint32_t s = (uint32_t)q * kPrRange;
+	const uint32_t s = (uint32_t)q * kMapRange;
 	// last entry e with pos[e] <= s (pos[0] = 0 <= s)
-	uint32_t lo = 0, hi = (uint32_t)a.sp.in.V;
+	uint32_t lo = 0, hi = (uint32_t)a.sp.g.V;
 	while (lo < hi) {
 		const uint32_t mid = (lo + hi + 1) >> 1;
 		if (__ldg(a.sp.pos + mid) <= s) lo = mid; else hi = mid - 1;
 	}
 	const uint32_t e = lo;
-	if (e >= a.sp.in.V) return;
+	if (e >= a.sp.g.V) return;
 	const uint32_t start = __ldg(a.sp.pos + e), end = __ldg(a.sp.pos + e + 1);
-	if (!(start < s && start >= s - kPrRange && end > s)) return;
-	const uint32_t r2 = (end - 1) / kPrRange;
+	if (!(start < s && start >= s - kMapRange && end > s)) return;
+	const uint32_t r2 = (end - 1) / kMapRange;
 	double t = __ldcg(a.carry_last + (q - 1));
 	for (uint32_t x = (uint32_t)q; x <= r2; x++) t += __ldcg(a.carry_first + x);
 	pr_finish(a, e, t);
@@ -607,16 +352,6 @@ __global__ void pr_init(const uint32_t* outdeg, uint64_t V, double pr0,
 	uint32_t dg = outdeg[v];
 	contrib[v] = dg ? pr0 / (double)dg : 0.0;
 	if (pr_out) pr_out[v] = pr0;
-}
-
-static SlotSpace slot_space(const lg_snapshot* sn) {
-	SlotSpace sp;
-	sp.in = sn->view(1);
-	sp.pos = sn->in.slot_off.as<uint32_t>();
-	sp.range_lb = sn->in.range_lb.as<uint32_t>();
-	sp.total = (uint32_t)sn->in.n_frag_slots;
-	sp.nranges = (uint32_t)std::max<uint64_t>(1, (sp.total + kPrRange - 1) / kPrRange);
-	return sp;
 }
 
 static lg_status check_args(lg_snapshot* sn, int iterations, double damping, double* ranks) {
@@ -645,56 +380,29 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 	const double N = (double)V;
 	const double pr0 = 1.0 / N;
 	const double base = (1.0 - damping) / N;
-	const SlotSpace sp = slot_space(sn);
 	const unsigned B = 256;
 	DevBuf* sc = s->scratch;
 	const uint32_t* outdeg = sn->out.deg.as<uint32_t>();
 
-	// flat in-adjacency of the snapshot
-	LG_TRY(sc[7].reserve(2ull * (sp.nranges + 1) * sizeof(uint32_t)));
-	uint32_t* blk_live = sc[7].as<uint32_t>();
-	uint32_t* blk_base = blk_live + sp.nranges + 1;
-	flat_count<<<sp.nranges, kPrThreads, 0, st>>>(sp, blk_live);
-	LG_CUDA(cudaGetLastError(), "flat_count");
-	uint64_t E = 0;
-	LG_TRY(exclusive_scan_u32(blk_live, blk_base, sp.nranges, sc[8], st, &E));
-	if (E > 0xffffffffull - 2 * kFlatTile)
-		return set_error(LG_ENOTSUP, "more than 2^32 - %u live in-edges", 2 * kFlatTile);
-	const uint32_t ntiles = (uint32_t)((E + kFlatTile - 1) / kFlatTile);
-	LG_TRY(sc[3].reserve(std::max<uint64_t>(E, 1) * sizeof(uint32_t)));
-	LG_TRY(sc[5].reserve(2 * (V + 1) * sizeof(uint32_t)));
-	uint32_t* flat_off = sc[5].as<uint32_t>();
-	uint32_t* kidx = flat_off + V + 1;
-	flat_write<<<sp.nranges, kPrThreads, 0, st>>>(sp, blk_base, sc[3].as<uint32_t>(), flat_off);
-	LG_CUDA(cudaGetLastError(), "flat_write");
-	LG_TRY(sc[9].reserve(V * sizeof(uint32_t)));
-	flat_flags<<<grid_for(V, B), B, 0, st>>>(flat_off, V, sc[9].as<uint32_t>());
-	LG_CUDA(cudaGetLastError(), "flat_flags");
-	uint64_t R = 0;
-	LG_TRY(exclusive_scan_u32(sc[9].as<uint32_t>(), kidx, V, sc[8], st, &R));
-	const uint64_t head_words = (uint64_t)ntiles * kFlatTileWords + 1;
-	LG_TRY(sc[6].reserve((2 * std::max<uint64_t>(R, 1) + ntiles + head_words) * sizeof(uint32_t)));
-	uint32_t* nz_rows = sc[6].as<uint32_t>();
-	uint32_t* nz_off = nz_rows + std::max<uint64_t>(R, 1);
-	uint32_t* tile_seg = nz_off + std::max<uint64_t>(R, 1);
-	uint32_t* heads = tile_seg + ntiles;
-	LG_CUDA(cudaMemsetAsync(heads, 0, head_words * sizeof(uint32_t), st), "clear heads");
-	flat_rows<<<grid_for(V, B), B, 0, st>>>(flat_off, kidx, V, nz_rows, nz_off, heads);
-	LG_CUDA(cudaGetLastError(), "flat_rows");
-	if (ntiles > 0) {
-		flat_tiles<<<grid_for(ntiles, B), B, 0, st>>>(nz_off, (uint32_t)R, ntiles, tile_seg);
-		LG_CUDA(cudaGetLastError(), "flat_tiles");
+	// flat in-adjacency: the snapshot's own (lg_snapshot_flatten) or one
+	// built for this call in store scratch
+	const FlatCsr* f = sn->flat[1];
+	if (!f) {
+		if (!s->flat_scratch) s->flat_scratch = new FlatCsr;
+		LG_TRY(build_flat(sn, 1, *s->flat_scratch, false));
+		f = s->flat_scratch;
 	}
-	s->launches += 2 + 3 + 1 + 3 + 1 + (ntiles > 0);
+	const uint32_t ntiles = f->ntiles;
+	const uint32_t* flat_off = f->off.as<uint32_t>();
 
 	FlatArgs a;
-	a.ids = sc[3].as<uint32_t>();
-	a.heads = heads;
-	a.nz_rows = nz_rows;
-	a.nz_off = nz_off;
-	a.tile_seg = tile_seg;
-	a.E = (uint32_t)E;
-	a.R = (uint32_t)R;
+	a.ids = f->ids.as<uint32_t>();
+	a.heads = f->heads();
+	a.nz_rows = f->nz_rows();
+	a.nz_off = f->nz_off();
+	a.tile_seg = f->tile_seg();
+	a.E = (uint32_t)f->E;
+	a.R = (uint32_t)f->R;
 	a.ntiles = ntiles;
 	a.outdeg = outdeg;
 	a.base = base;
@@ -775,7 +483,7 @@ extern "C" lg_status lg_pagerank_pull_noalloc(lg_snapshot* sn, int iterations,
 	LG_TRY(check_args(sn, iterations, damping, ranks));
 	lg_store* s = sn->store;
 	const uint64_t V = sn->V;
-	const SlotSpace sp = slot_space(sn);
+	const SlotSpace sp = slot_space(sn, 1);
 	const uint64_t nranges = sp.nranges;
 	// contrib (two vectors), the result staged for host outputs, carries
 	const uint64_t need = 3 * V * sizeof(double) + 2 * nranges * sizeof(double);
@@ -783,7 +491,7 @@ extern "C" lg_status lg_pagerank_pull_noalloc(lg_snapshot* sn, int iterations,
 		return set_error(LG_EINVAL, "graph needs %llu scratch bytes, more than the %llu "
 				"this entry point has (24 B per vertex + 16 B per %u in-CSR slots)",
 				(unsigned long long)need, (unsigned long long)LG_NOALLOC_SCRATCH_BYTES,
-				kPrRange);
+				kMapRange);
 	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
 	// Device address of the scratch array, looked up once per device with
 	// that device current (host code must not use the symbol itself).
@@ -823,7 +531,7 @@ extern "C" lg_status lg_pagerank_pull_noalloc(lg_snapshot* sn, int iterations,
 		a.contrib = (it & 1) ? c1 : c0;
 		a.contrib_next = (it & 1) ? c0 : c1;
 		a.pr_out = (it == iterations - 1) ? pr_buf : nullptr;
-		pr_pull_step<<<nranges, kPrThreads, 0, st>>>(a);
+		pr_pull_step<<<nranges, kMapThreads, 0, st>>>(a);
 		if (nranges > 1) pr_fixup<<<grid_for(nranges, 256), 256, 0, st>>>(a);
 	}
 	LG_CUDA(cudaGetLastError(), "pagerank noalloc");

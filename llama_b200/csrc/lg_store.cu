@@ -2,6 +2,7 @@
 // the reference's layout, snapshot views (fragment walk + deletion bitset),
 // degree and adjacency queries, and the error plumbing of the C ABI.
 #include "lg_device.cuh"
+#include "lg_flat.cuh"
 
 #include <omp.h>
 
@@ -641,6 +642,8 @@ lg_status lg_store_destroy(lg_store* s) {
 	cudaStreamSynchronize(s->stream);
 	for (int i = 0; i < 2; i++) if (s->staged[i]) cudaEventDestroy(s->staged[i]);
 	if (s->pinned) cudaFreeHost(s->pinned);
+	delete s->flat_scratch;
+	for (int d = 0; d < 2; d++) delete s->flat_spare[d];
 	if (s->own_stream) cudaStreamDestroy(s->stream);
 	delete s;
 	return LG_OK;
@@ -754,7 +757,7 @@ lg_status lg_snapshot_get_stats(const lg_snapshot* sn, int dir, lg_snapshot_stat
 	st->slots = d.n_slots;
 	st->fragment_slots = d.n_frag_slots;
 	st->fragments = d.n_frags;
-	st->ranges = (d.n_frag_slots + 2047) / 2048;
+	st->ranges = (d.n_frag_slots + kBlockSlots - 1) / kBlockSlots;
 	st->deletions = d.n_dels;
 	return LG_OK;
 }
@@ -787,6 +790,7 @@ lg_status lg_snapshot_close(lg_snapshot* sn) {
 	cudaStreamSynchronize(sn->store->stream);
 	sn->store->open_snapshots--;
 	if (sn->adj_maps) lg_free_adjoint_maps(sn->adj_maps);
+	for (int d = 0; d < 2; d++) lg_flat_release(sn->store, sn->flat[d]);
 	delete sn;
 	return LG_OK;
 }

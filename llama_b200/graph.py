@@ -290,6 +290,21 @@ class Snapshot:
             return off, nb[:n], ei[:n]
         return off, nb[:n]
 
+    def flatten(self, direction=1):
+        """Keep direction `direction` (0 out, 1 in) as one flat CSR on the
+        device; traversals of it on this snapshot read that instead."""
+        check(lib.lg_snapshot_flatten(self._h, int(direction)))
+        return self
+
+    def unflatten(self):
+        check(lib.lg_snapshot_unflatten(self._h))
+        return self
+
+    def is_flat(self, direction=1):
+        f = C.c_int()
+        check(lib.lg_snapshot_is_flat(self._h, int(direction), C.byref(f)))
+        return bool(f.value)
+
     # ---- benchmark tasks -------------------------------------------------
     def pagerank_pull(self, iterations=10, damping=0.85, out=None):
         """Task ``pagerank_double``: FP64 pull PageRank."""
