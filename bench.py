@@ -328,46 +328,8 @@ def run_lg(args):
     e2e = None
     if not args.no_e2e:
         sn.close()
-        pr_host = torch.empty(V, dtype=torch.float64).pin_memory()
-        lv_host = torch.empty((len(roots), V), dtype=torch.int32).pin_memory()
-        L = hg.num_levels - 1
-        desc = hg.level_desc(L)
-
-        def e2e_step():
-            st.drop_level()
-            st.ingest_level(desc)
-            s2 = st.snapshot()
-            s2.flatten(1)
-            s2.pagerank_pull(args.pr_iters, 0.85, out=pr_host)
-            reach = 0
-            for i, r in enumerate(roots):
-                _, res = s2.bfs(int(r), out=lv_host[i])
-                reach += res.reach_edges
-            s2.close()
-            return reach
-        e2e_step()
-        st.sync()
-        barrier(ws)
-        h0, d0 = st.transfer_bytes()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e2e_edges = 0
-        e0.record(stream)
-        for _ in range(args.steps):
-            e2e_edges += args.pr_iters * E + e2e_step()
-        e1.record(stream)
-        stream.synchronize()
-        h1, d1 = st.transfer_bytes()
-        e2e_ms = e0.elapsed_time(e1)
-        e2e_ms_max, e2e_edges_all = reduce_max_sum(ws, e2e_ms, e2e_edges)
-        e2e = {"value": e2e_edges_all / (e2e_ms_max / 1e3) / 1e9, "unit": "GTEPS",
-               "h2d_bytes_per_step": (h1 - h0) // args.steps,
-               "d2h_bytes_per_step": (d1 - d0) // args.steps,
-               "ms_per_step": e2e_ms_max / args.steps,
-               "includes": "ingest of the newest level from host + snapshot open + "
-                           "in-CSR flatten + PageRank + BFS with results copied to "
-                           "pinned host memory"}
         sn = None
+        e2e = run_e2e(args, ws, st, hg, V, E, roots, stream)
 
     ext = None
     if not args.no_extras:
@@ -404,6 +366,98 @@ def run_lg(args):
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def run_e2e(args, ws, st, hg, V, E, roots, stream):
+    """The step through the C ABI with host buffers: every step replaces the
+    newest level (dropped, then rebuilt on the device from its edge delta in
+    pinned host memory with lg_store_build_level), opens the snapshot,
+    flattens its in-CSR, and copies the ranks and BFS levels to pinned host
+    memory.  The same with the host-built level ingested through
+    lg_store_ingest_level is reported as host_level.  Then one more step with
+    a synchronisation after each phase gives the breakdown."""
+    import torch
+    pr_host = torch.empty(V, dtype=torch.float64).pin_memory()
+    lv_host = torch.empty((len(roots), V), dtype=torch.int32).pin_memory()
+    L = hg.num_levels - 1
+    desc = hg.level_desc(L)
+    src, dst, dsrc, ddst, w = hg.level_input(L)
+
+    def pin(a):
+        return None if a is None else torch.from_numpy(a.view(np.int32)).pin_memory()
+    p_src, p_dst, p_dsrc, p_ddst, p_w = (pin(x) for x in (src, dst, dsrc, ddst, w))
+
+    def load(kind):
+        st.drop_level()
+        if kind == "device":
+            st.build_level(V, p_src, p_dst, p_w, p_dsrc, p_ddst)
+        else:
+            st.ingest_level(desc)
+
+    def analytics(phase=None):
+        s2 = st.snapshot()
+        if phase:
+            phase("snapshot_open")
+        s2.flatten(1)
+        s2.pagerank_pull(args.pr_iters, 0.85, out=pr_host)
+        if phase:
+            phase("flatten_pagerank_to_host")
+        reach = 0
+        for i, r in enumerate(roots):
+            _, res = s2.bfs(int(r), out=lv_host[i])
+            reach += res.reach_edges
+        if phase:
+            phase("bfs_to_host")
+        s2.close()
+        return reach
+
+    def measure(kind):
+        load(kind)
+        analytics()
+        st.sync()
+        barrier(ws)
+        h0, d0 = st.transfer_bytes()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        edges = 0
+        e0.record(stream)
+        for _ in range(args.steps):
+            load(kind)
+            edges += args.pr_iters * E + analytics()
+        e1.record(stream)
+        stream.synchronize()
+        h1, d1 = st.transfer_bytes()
+        ms = e0.elapsed_time(e1)
+        ms_max, edges_all = reduce_max_sum(ws, ms, edges)
+        return {"value": edges_all / (ms_max / 1e3) / 1e9, "unit": "GTEPS",
+                "h2d_bytes_per_step": (h1 - h0) // args.steps,
+                "d2h_bytes_per_step": (d1 - d0) // args.steps,
+                "ms_per_step": ms_max / args.steps}
+
+    out = measure("device")
+    out["includes"] = ("newest level rebuilt on the device from its edge delta (pinned host "
+                       "arrays) + snapshot open + in-CSR flatten + PageRank + BFS with "
+                       "results copied to pinned host memory")
+    host = measure("host")
+    host["includes"] = "as above, the level built on the host and ingested"
+    out["host_level"] = host
+    # phase breakdown of one more device-built step (host clock, synchronised)
+    phases = {}
+    t = [time.perf_counter()]
+
+    def phase(name):
+        st.sync()
+        now = time.perf_counter()
+        phases[name] = (now - t[0]) * 1e3
+        t[0] = now
+    st.drop_level()
+    st.sync()
+    t[0] = time.perf_counter()
+    st.build_level(V, p_src, p_dst, p_w, p_dsrc, p_ddst)
+    phase("build_level")
+    analytics(phase)
+    out["phases_ms"] = phases
+    return out
 
 
 def _timed(stream, fn):

@@ -174,6 +174,36 @@ lg_status lg_store_transfer_bytes(const lg_store* store, uint64_t* h2d,
  * LG_ESTATE while snapshots are open. */
 lg_status lg_store_drop_level(lg_store* store);
 
+/* Build the next level on the device from its edge delta instead of
+ * ingesting a level the host built: the vertex tables and edge slots come out
+ * as ll_mlcsr_core::init_level_from_degrees / init_node / write_values /
+ * finish_level_vertices (llama/include/llama/ll_mlcsr_sp.h:1375-1715) and,
+ * for the in-CSR, make_reverse_edges (llama/include/llama/ll_mlcsr_graph.h:
+ * 955-1058) lay them out (new edges sorted by (source, target) within a
+ * vertex), identical to that level ingested with lg_store_ingest_level; each
+ * deleted edge gets its max_visible_level lowered to the new level in the
+ * older slot that holds it live (ll_writable_graph.h:936-945).
+ *   max_nodes      vertices of the level (>= the previous level's)
+ *   src, dst       n_new new edges, any order; no duplicates, none live in
+ *                  the previous snapshot
+ *   weights        uint32 per new edge, the out-CSR's edge property, or NULL
+ *   del_src/dst    n_del edges live in the previous snapshot to delete
+ *                  (none at level 0)
+ * Arrays may be host or device memory.  On any error the store is unchanged. */
+lg_status lg_store_build_level(lg_store* store, uint64_t max_nodes,
+		const uint32_t* src, const uint32_t* dst, const uint32_t* weights,
+		uint64_t n_new, const uint32_t* del_src, const uint32_t* del_dst,
+		uint64_t n_del);
+
+/* Copy level `level` of direction dir (0 out, 1 in) as the device holds it:
+ * vt = lg_vt_entry[max_nodes + 1], ids = uint32[n_slots] (the payload of
+ * every fragment slot, 0xffffffff elsewhere: continuation records, unused
+ * space), weights = uint32[n_slots] (LG_ESTATE if the level has none).  Any
+ * output may be NULL; *n_slots (if not NULL) receives the slot count.  No
+ * reference counterpart: a readback for checking levels built on the device. */
+lg_status lg_store_read_level(lg_store* store, int level, int dir, lg_vt_entry* vt,
+		uint32_t* ids, uint32_t* weights, uint64_t* n_slots);
+
 /* ---------------------------------------------------------------------------
  * Snapshots.  A read-only view whose latest level is `level`, with deletions
  * filtered at max_level = level: the snapshot constructor

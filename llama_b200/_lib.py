@@ -127,6 +127,8 @@ SIGNATURES = [
     ("lg_store_launch_count", _U64, [_P]),
     ("lg_store_transfer_bytes", _INT, [_P, C.POINTER(_U64), C.POINTER(_U64)]),
     ("lg_store_drop_level", _INT, [_P]),
+    ("lg_store_build_level", _INT, [_P, _U64, _P, _P, _P, _U64, _P, _P, _U64]),
+    ("lg_store_read_level", _INT, [_P, _INT, _INT, _P, _P, _P, C.POINTER(_U64)]),
     ("lg_snapshot_get_stats", _INT, [_P, _INT, C.POINTER(lg_snapshot_stats)]),
     ("lg_snapshot_open", _INT, [_P, _INT, _PP]),
     ("lg_snapshot_close", _INT, [_P]),

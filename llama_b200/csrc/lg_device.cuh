@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
 #include <vector>
 
 #include "lg_internal.h"
@@ -147,6 +148,7 @@ struct DevBuf {
 	// (Re)allocate to at least n bytes; contents are not preserved.
 	lg_status reserve(size_t n);
 	template <class T> T* as() const { return static_cast<T*>(p); }
+	void swap(DevBuf& o) { std::swap(p, o.p); std::swap(bytes, o.bytes); }
 };
 
 struct DevLevel {
@@ -173,12 +175,21 @@ constexpr uint32_t kBlockSlots = 1024;
 struct SnapDir {
 	DevBuf frag_off, frags, deg, delbits, lt, slot_off;
 	DevBuf range_lb;               // lower_bound(slot_off, r * kBlockSlots), r = 0..nblocks
+	DevBuf tmp_cnt, tmp_slots, tmp_scan, tmp_words, tmp_sum;   // open-time scratch
 	uint64_t n_frags = 0;
 	uint64_t n_edges = 0;          // live edges (sum of degrees)
 	uint64_t n_slots = 0;          // slots of levels 0..L
 	uint64_t n_frag_slots = 0;     // slots covered by fragments
 	uint64_t n_dels = 0;           // deletion marks visible at L
 	bool present = false;
+	// exchange device buffers with o (a closed snapshot's, kept for reuse)
+	void swap_buffers(SnapDir& o) {
+		DevBuf* a[] = {&frag_off, &frags, &deg, &delbits, &lt, &slot_off, &range_lb,
+			&tmp_cnt, &tmp_slots, &tmp_scan, &tmp_words, &tmp_sum};
+		DevBuf* b[] = {&o.frag_off, &o.frags, &o.deg, &o.delbits, &o.lt, &o.slot_off,
+			&o.range_lb, &o.tmp_cnt, &o.tmp_slots, &o.tmp_scan, &o.tmp_words, &o.tmp_sum};
+		for (size_t i = 0; i < sizeof(a) / sizeof(a[0]); i++) a[i]->swap(*b[i]);
+	}
 	SnapCsr view() const {
 		SnapCsr s;
 		s.frag_off = frag_off.as<uint32_t>();
@@ -212,6 +223,12 @@ struct lg_store {
 	uint64_t d2h_bytes = 0;     // device -> host bytes copied by this store
 	lg::FlatCsr* flat_scratch = nullptr;   // per-call flat in-CSR of PageRank
 	lg::FlatCsr* flat_spare[2] = {nullptr, nullptr};   // unflattened, kept for reuse
+	// device buffers of the last closed snapshot and the last dropped level,
+	// per direction, reused by the next open / level (the stream was
+	// synchronised when they were released)
+	lg::SnapDir* snap_spare[2] = {nullptr, nullptr};
+	lg::DevLevel* level_spare[2] = {nullptr, nullptr};
+	lg::DevBuf build_tmp[12];   // lg_store_build_level temporaries
 };
 
 // Edge-order maps of a snapshot used by the differentiable PageRank
@@ -252,6 +269,15 @@ lg_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n,
 // Copy `bytes` of device data to a caller buffer (host or device) on the
 // store's stream, counting host-bound bytes.
 lg_status copy_out(lg_store* s, void* dst, const void* src, size_t bytes);
+
+// A DevLevel for direction dir (0 out, 1 in) of a new level: the store's
+// spare (buffers of the last dropped level) or a new one.  Null if the host
+// allocation fails.
+DevLevel* take_level(lg_store* s, int dir);
+
+// Brings the device deletion list of csr up to its host mirror, whose first
+// old_n entries the device copy already holds.
+lg_status upload_dels(lg_store* s, DevCsr& csr, size_t old_n);
 
 inline unsigned grid_for(uint64_t n, unsigned block) {
 	uint64_t g = (n + block - 1) / block;

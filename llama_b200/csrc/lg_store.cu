@@ -65,6 +65,36 @@ lg_status copy_out(lg_store* s, void* dst, const void* src, size_t bytes) {
 	return LG_OK;
 }
 
+DevLevel* take_level(lg_store* s, int dir) {
+	DevLevel* d = s->level_spare[dir];
+	s->level_spare[dir] = nullptr;
+	if (!d) return new (std::nothrow) DevLevel();
+	d->max_nodes = d->n_slots = d->n_fragment_slots = 0;
+	return d;
+}
+
+lg_status upload_dels(lg_store* s, DevCsr& csr, size_t old_n) {
+	const size_t n = csr.dels_host.size();
+	if (n == 0) { csr.n_dels_dev = 0; return LG_OK; }
+	const size_t need = n * sizeof(uint2);
+	size_t from = std::min(old_n, csr.n_dels_dev);
+	if (need > csr.dels.bytes) {
+		// the previous device copy may still be read by queued kernels
+		LG_CUDA(cudaStreamSynchronize(s->stream), "deletion list");
+		LG_TRY(csr.dels.reserve(need + need / 2));
+		from = 0;
+	}
+	if (n > from) {
+		// pageable source: the copy completes before cudaMemcpyAsync returns
+		LG_CUDA(cudaMemcpyAsync(csr.dels.as<uint2>() + from, csr.dels_host.data() + from,
+				(n - from) * sizeof(uint2), cudaMemcpyHostToDevice, s->stream),
+				"deletion list");
+		s->h2d_bytes += (n - from) * sizeof(uint2);
+	}
+	csr.n_dels_dev = n;
+	return LG_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Exclusive scan (u32 -> u32): per-tile sums, a single-CTA scan of the tile
 // sums, then per-tile scans with the carried offset.
@@ -256,11 +286,12 @@ static lg_status ingest_csr(lg_store* s, DevCsr& csr, int l,
 	if (bad & 1) return set_error(LG_EINVAL, "%s: vertex table points to a future level", name);
 	if (bad & 2) return set_error(LG_EINVAL, "%s: fragment exceeds its edge table", name);
 
-	DevLevel* d = new (std::nothrow) DevLevel();
+	DevLevel* d = take_level(s, &csr == &s->out ? 0 : 1);
 	if (!d) return set_error(LG_ENOMEM, "host allocation");
 	d->max_nodes = V;
 	d->n_slots = S;
 	d->n_fragment_slots = frag_slots;
+	if (!c.weights) d->w.release();
 	lg_status st = d->vt.reserve((V + 1) * sizeof(lg_vt_entry));
 	if (!st) st = d->ids.reserve(std::max<uint64_t>(S, 1) * sizeof(uint32_t));
 	if (!st && c.weights) st = d->w.reserve(std::max<uint64_t>(S, 1) * sizeof(uint32_t));
@@ -331,24 +362,11 @@ static lg_status ingest_csr(lg_store* s, DevCsr& csr, int l,
 		}
 		add.push_back(make_uint2((uint32_t)ix, (el << LG_BITS_LEVEL) | x.max_visible_level));
 	}
-	csr.dels_mark.push_back(csr.dels_host.size());
+	const size_t old_n = csr.dels_host.size();
+	csr.dels_mark.push_back(old_n);
 	csr.levels.push_back(d);
 	csr.dels_host.insert(csr.dels_host.end(), add.begin(), add.end());
-	if (!csr.dels_host.empty()) {
-		size_t need = csr.dels_host.size() * sizeof(uint2);
-		if (need > csr.dels.bytes) {
-			// the previous device copy may still be read by queued kernels
-			LG_CUDA(cudaStreamSynchronize(s->stream), "ingest sync");
-			LG_TRY(csr.dels.reserve(need + need / 2));
-		}
-		LG_CUDA(cudaMemcpyAsync(csr.dels.p, csr.dels_host.data(), need,
-				cudaMemcpyHostToDevice, s->stream), "deletion list");
-		s->h2d_bytes += need;
-		// the host vector must outlive the async copy from pageable memory;
-		// pageable copies complete before cudaMemcpyAsync returns
-		csr.n_dels_dev = csr.dels_host.size();
-	}
-	return LG_OK;
+	return upload_dels(s, csr, old_n);
 }
 
 // ---------------------------------------------------------------------------
@@ -387,15 +405,22 @@ __global__ void walk_fragments(VtTab tab, int L, uint64_t V, uint32_t* count,
 	if (!kFill) { count[v] = n; slots_per_vertex[v] = slots; }
 }
 
+// Sets the bit of every slot deleted at or before L and counts them in *count.
 __global__ void mark_deletions(const uint2* dels, uint64_t n, int L,
-		uint32_t* const* del_words) {
+		uint32_t* const* del_words, unsigned long long* count) {
 	uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= n) return;
-	uint2 d = dels[i];
-	uint32_t lv = d.y >> LG_BITS_LEVEL;
-	uint32_t ml = d.y & ((1u << LG_BITS_LEVEL) - 1u);
-	if ((int)lv > L || (int)ml > L) return;
-	atomicOr(del_words[lv] + (d.x >> 5), 1u << (d.x & 31));
+	bool hit = false;
+	if (i < n) {
+		uint2 d = dels[i];
+		uint32_t lv = d.y >> LG_BITS_LEVEL;
+		uint32_t ml = d.y & ((1u << LG_BITS_LEVEL) - 1u);
+		if ((int)lv <= L && (int)ml <= L) {
+			atomicOr(del_words[lv] + (d.x >> 5), 1u << (d.x & 31));
+			hit = true;
+		}
+	}
+	const unsigned m = __ballot_sync(0xffffffffu, hit);
+	if ((threadIdx.x & 31u) == 0 && m) atomicAdd(count, (unsigned long long)__popc(m));
 }
 
 // lb[r] = first vertex e with pos[e] >= r * kBlockSlots (pos has V + 1
@@ -425,6 +450,8 @@ __global__ void sum_u32(const uint32_t* x, uint64_t n, unsigned long long* out) 
 static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 	lg_store* s = sn->store;
 	const int L = sn->level;
+	SnapDir*& spare = s->snap_spare[&csr == &s->out ? 0 : 1];
+	if (spare) d.swap_buffers(*spare);       // a closed snapshot's device buffers
 	const uint64_t V = csr.levels[L]->max_nodes;
 	cudaStream_t st = s->stream;
 	VtTab tab;
@@ -433,7 +460,9 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 		tab.vt[l] = csr.levels[l]->vt.as<lg_vt_entry>();
 		tab.max_nodes[l] = csr.levels[l]->max_nodes;
 	}
-	DevBuf cnt, slots, scan_tmp;
+	DevBuf& cnt = d.tmp_cnt;
+	DevBuf& slots = d.tmp_slots;
+	DevBuf& scan_tmp = d.tmp_scan;
 	LG_TRY(cnt.reserve(V * sizeof(uint32_t)));
 	LG_TRY(slots.reserve(V * sizeof(uint32_t)));
 	LG_TRY(d.deg.reserve(V * sizeof(uint32_t)));
@@ -470,17 +499,19 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 	LG_TRY(d.lt.reserve(sizeof(LevelTab)));
 	LG_CUDA(cudaMemcpyAsync(d.lt.p, &lt, sizeof(lt), cudaMemcpyHostToDevice, st),
 			"level table");
+	DevBuf& counters = d.tmp_sum;     // [0] live degree sum, [1] deletions visible at L
+	LG_TRY(counters.reserve(2 * sizeof(unsigned long long)));
+	LG_CUDA(cudaMemsetAsync(counters.p, 0, 2 * sizeof(unsigned long long), st), "memset");
 	if (csr.n_dels_dev > 0) {
-		DevBuf words;
+		DevBuf& words = d.tmp_words;
 		LG_TRY(words.reserve(sizeof(uint32_t*) * LG_MAX_LEVELS));
 		LG_CUDA(cudaMemcpyAsync(words.p, lt.del, sizeof(lt.del),
 				cudaMemcpyHostToDevice, st), "deletion table");
 		mark_deletions<<<grid_for(csr.n_dels_dev, B), B, 0, st>>>(
 				csr.dels.as<uint2>(), csr.n_dels_dev, L,
-				(uint32_t* const*)words.p);
+				(uint32_t* const*)words.p, counters.as<unsigned long long>() + 1);
 		LG_CUDA(cudaGetLastError(), "mark_deletions");
 		s->launches++;
-		LG_CUDA(cudaStreamSynchronize(st), "snapshot deletions");
 	}
 
 	// per-vertex slot prefix (the virtual slot space the balanced kernels cut
@@ -497,24 +528,17 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 		LG_CUDA(cudaGetLastError(), "block_lower_bounds");
 		s->launches++;
 	}
-	DevBuf counters;
-	LG_TRY(counters.reserve(sizeof(unsigned long long)));
-	LG_CUDA(cudaMemsetAsync(counters.p, 0, sizeof(unsigned long long), st), "memset");
 	sum_u32<<<592, B, 0, st>>>(d.deg.as<uint32_t>(), V, counters.as<unsigned long long>());
 	LG_CUDA(cudaGetLastError(), "degree sum");
 	s->launches += 4;
-	unsigned long long ne = 0;
-	LG_CUDA(cudaMemcpyAsync(&ne, counters.p, sizeof(ne), cudaMemcpyDeviceToHost, st), "d2h");
+	unsigned long long sums[2] = {0, 0};
+	LG_CUDA(cudaMemcpyAsync(sums, counters.p, sizeof(sums), cudaMemcpyDeviceToHost, st), "d2h");
 	LG_CUDA(cudaStreamSynchronize(st), "snapshot sizes");
-	d.n_edges = ne;
+	d.n_edges = sums[0];
 	d.n_frag_slots = total_slots;
 	d.n_slots = 0;
 	for (int l = 0; l <= L; l++) d.n_slots += csr.levels[l]->n_slots;
-	d.n_dels = 0;
-	for (const uint2& x : csr.dels_host) {
-		uint32_t lv = x.y >> LG_BITS_LEVEL, ml = x.y & ((1u << LG_BITS_LEVEL) - 1u);
-		d.n_dels += ((int)lv <= L && (int)ml <= L);
-	}
+	d.n_dels = sums[1];
 	d.present = true;
 	return LG_OK;
 }
@@ -643,7 +667,11 @@ lg_status lg_store_destroy(lg_store* s) {
 	for (int i = 0; i < 2; i++) if (s->staged[i]) cudaEventDestroy(s->staged[i]);
 	if (s->pinned) cudaFreeHost(s->pinned);
 	delete s->flat_scratch;
-	for (int d = 0; d < 2; d++) delete s->flat_spare[d];
+	for (int d = 0; d < 2; d++) {
+		delete s->flat_spare[d];
+		delete s->snap_spare[d];
+		delete s->level_spare[d];
+	}
 	if (s->own_stream) cudaStreamDestroy(s->stream);
 	delete s;
 	return LG_OK;
@@ -734,9 +762,11 @@ lg_status lg_store_drop_level(lg_store* s) {
 		return set_error(LG_ESTATE, "close all snapshots before dropping a level");
 	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
 	LG_CUDA(cudaStreamSynchronize(s->stream), "drop level");
-	for (DevCsr* c : {&s->out, &s->in}) {
+	for (int dir = 0; dir < 2; dir++) {
+		DevCsr* c = dir == 0 ? &s->out : &s->in;
 		if (c->levels.empty()) continue;
-		delete c->levels.back();
+		delete s->level_spare[dir];               // keep the newest dropped level's buffers
+		s->level_spare[dir] = c->levels.back();
 		c->levels.pop_back();
 		// the device copy keeps the same prefix of the list
 		c->dels_host.resize(c->dels_mark.back());
@@ -791,6 +821,14 @@ lg_status lg_snapshot_close(lg_snapshot* sn) {
 	sn->store->open_snapshots--;
 	if (sn->adj_maps) lg_free_adjoint_maps(sn->adj_maps);
 	for (int d = 0; d < 2; d++) lg_flat_release(sn->store, sn->flat[d]);
+	// keep this snapshot's device buffers for the next open
+	lg_store* s = sn->store;
+	for (int d = 0; d < 2; d++) {
+		SnapDir& sd = d == 0 ? sn->out : sn->in;
+		if (!sd.present) continue;
+		if (!s->snap_spare[d]) s->snap_spare[d] = new (std::nothrow) SnapDir();
+		if (s->snap_spare[d]) s->snap_spare[d]->swap_buffers(sd);
+	}
 	delete sn;
 	return LG_OK;
 }

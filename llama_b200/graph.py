@@ -185,6 +185,39 @@ class Store:
         check(lib.lg_store_transfer_bytes(self._h, C.byref(h), C.byref(d)))
         return h.value, d.value
 
+    def build_level(self, max_nodes, src, dst, weights=None, del_src=(), del_dst=()):
+        """Build the next level on the device from its edge delta
+        (``lg_store_build_level``).  Arrays may be numpy (host) or torch CUDA
+        tensors of uint32/int32."""
+        def arr(a):
+            if hasattr(a, "data_ptr"):
+                return a, a.numel()
+            a = _u32(a)
+            return a, len(a)
+        s, n = arr(src)
+        d, _ = arr(dst)
+        ds, nd = arr(del_src)
+        dd, _ = arr(del_dst)
+        w = None if weights is None else arr(weights)[0]
+        check(lib.lg_store_build_level(self._h, int(max_nodes), ptr(s), ptr(d), ptr(w), n,
+                                       ptr(ds) if nd else None, ptr(dd) if nd else None, nd))
+
+    def read_level(self, level, direction=0, weights=False):
+        """(vertex table, ids[, weights]) of a level as the device holds it."""
+        n = C.c_uint64()
+        check(lib.lg_store_read_level(self._h, level, direction, None, None, None, C.byref(n)))
+        mn = C.c_uint64()
+        check(lib.lg_store_max_nodes(self._h, level, C.byref(mn)))
+        vt = np.empty(mn.value + 1, _lib.VT_DTYPE)
+        ids = np.empty(max(n.value, 1), np.uint32)
+        w = np.empty(max(n.value, 1), np.uint32) if weights else None
+        check(lib.lg_store_read_level(self._h, level, direction, ptr(vt), ptr(ids), ptr(w),
+                                      None))
+        ids = ids[:n.value]
+        if weights:
+            return vt, ids, w[:n.value]
+        return vt, ids
+
     def snapshot(self, level=-1):
         return Snapshot(self, level)
 
