@@ -307,7 +307,8 @@ def run_lg(args):
     launch_s = statistics.median(diffs) / 1e3
     peak, peak_kind = measured_peak()
     achieved = pr_bytes / launch_s / 1e9
-    traffic = profiled_traffic()
+    # the committed ncu figure is for the default workload only
+    traffic = profiled_traffic() if (args.scale, args.levels) == (24, 8) else None
     roofline = {"bound": "hbm", "kernel": "pr_flat_step", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
@@ -322,7 +323,10 @@ def run_lg(args):
                 "launch_ms_source": "CUDA events on the store's stream: "
                                     "(t(2k iterations) - t(k iterations)) / k, median of 3",
                 "pr_call_ms": pr_ms / args.steps,
-                "traffic": traffic["dram_bytes_per_launch_scaled"] if traffic else None}
+                "traffic": traffic["dram_bytes_per_launch_scaled"] if traffic else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one "
+                                  "full-size launch (profiles/pr_flat_step_rmat24.md)"
+                                  if traffic else None}
 
     # e2e: newest level re-ingested from host, snapshot reopened, results to host
     e2e = None
