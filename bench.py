@@ -511,6 +511,14 @@ def extras(args, st, stream, device):
             tc, ms = _timed(stream, sn.triangle_count)
             res["triangle_count"] = {"ms": ms, "triangles": tc.triangles,
                                      "gteps": E / (ms / 1e3) / 1e9}
+            age = torch.randint(0, 80, (V,), dtype=torch.int32, device=dev,
+                                generator=torch.Generator(device=dev).manual_seed(16))
+            tcnt = torch.empty(V, dtype=torch.int32, device=dev)
+            sn.avg_teen_cnt(age, 0, out=tcnt)
+            (_, trr), ms = _timed(stream, lambda: sn.avg_teen_cnt(age, 0, out=tcnt))
+            res["avg_teen_cnt"] = {"ms": ms, "average": trr.average,
+                                   "gteps": E / (ms / 1e3) / 1e9,
+                                   "includes": "in-CSR flatten for the call"}
             lab = torch.empty(V, dtype=torch.int64, device=dev)
             sn.scc(out=lab)
             (_, sr), ms = _timed(stream, lambda: sn.scc(out=lab))

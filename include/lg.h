@@ -377,6 +377,24 @@ typedef struct lg_scc_result {
 
 lg_status lg_scc(lg_snapshot* snap, int64_t* labels, lg_scc_result* result);
 
+/* Task "avg_teen_cnt" (ll_b_avg_teen_cnt::run,
+ * benchmark/benchmarks/avg_teen_cnt.h:96-139): for every vertex n,
+ * teen_cnt[n] = number of in-neighbours t with 10 <= age[t] < 20; over the
+ * vertices with age[n] > K, average = (float)(sum of teen_cnt / count), 0 if
+ * none.  age: int32[max_nodes], the node property "age" of the snapshot
+ * (host or device memory); teen_cnt: int32[max_nodes] output, or NULL.  The
+ * reference accumulates the sum in int32; teen_sum here is 64-bit (equal
+ * while the sum fits 31 bits).  Requires the in-CSR; uses the snapshot's flat
+ * in-CSR when lg_snapshot_flatten made one. */
+typedef struct lg_teen_result {
+	double   average;     /* (float)(teen_sum / vertices), as the task returns it */
+	int64_t  teen_sum;    /* sum of teen_cnt over vertices with age > K */
+	int64_t  vertices;    /* vertices with age > K */
+} lg_teen_result;
+
+lg_status lg_avg_teen_cnt(lg_snapshot* snap, const int32_t* age, int K,
+		int32_t* teen_cnt, lg_teen_result* result);
+
 /* Brandes betweenness centrality from explicit sources: the kernel of task
  * "bc_random" (ll_b_bc_random::run, benchmark/benchmarks/bc_random.h:158-193,
  * bc_random_bfs :55-116) with the sources given instead of drawn by

@@ -80,6 +80,10 @@ class lg_tc_result(C.Structure):
                 ("arcs", C.c_uint64)]
 
 
+class lg_teen_result(C.Structure):
+    _fields_ = [("average", C.c_double), ("teen_sum", C.c_int64), ("vertices", C.c_int64)]
+
+
 class lg_scc_result(C.Structure):
     _fields_ = [("components", C.c_uint64), ("trimmed", C.c_uint64),
                 ("rounds", C.c_int32), ("steps", C.c_int32)]
@@ -146,6 +150,7 @@ SIGNATURES = [
     ("lg_bfs", _INT, [_P, _I64, _P, C.POINTER(lg_bfs_result)]),
     ("lg_sssp_delta", _INT, [_P, _I64, C.c_uint32, _P, C.POINTER(lg_sssp_result)]),
     ("lg_triangle_count", _INT, [_P, C.POINTER(lg_tc_result)]),
+    ("lg_avg_teen_cnt", _INT, [_P, _P, _INT, _P, C.POINTER(lg_teen_result)]),
     ("lg_scc", _INT, [_P, _P, C.POINTER(lg_scc_result)]),
     ("lg_bc", _INT, [_P, _P, _INT, _P]),
     ("lg_bc_batched", _INT, [_P, _P, _INT, _P]),

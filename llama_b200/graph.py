@@ -388,6 +388,15 @@ class Snapshot:
         check(lib.lg_triangle_count(self._h, C.byref(r)))
         return r
 
+    def avg_teen_cnt(self, age, K=0, out=None):
+        """Task ``avg_teen_cnt``: (teen_cnt per vertex, lg_teen_result).  age:
+        int32 per vertex (numpy or a torch CUDA tensor)."""
+        a = age if hasattr(age, "data_ptr") else np.ascontiguousarray(age, dtype=np.int32)
+        res = np.empty(self.max_nodes, np.int32) if out is None else out
+        r = _lib.lg_teen_result()
+        check(lib.lg_avg_teen_cnt(self._h, ptr(a), int(K), ptr(res), C.byref(r)))
+        return res, r
+
     def sssp(self, root, delta=32, out=None):
         """Task ``sssp_weighted`` (delta-stepping); returns (dist, lg_sssp_result)."""
         res = np.empty(self.max_nodes, np.uint32) if out is None else out

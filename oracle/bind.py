@@ -48,6 +48,8 @@ def lgo():
             ("lgo_bc", None, [_P, _INT, _P, _INT, _P]),
             ("lgo_sssp", _U64, [_P, _INT, _I64, _P]),
             ("lgo_tc", _I64, [_P, _INT]),
+            ("lgo_avg_teen_cnt", _D, [_P, _INT, _P, _INT, _P, C.POINTER(_I64),
+                                      C.POINTER(_I64)]),
             ("lgo_scc", None, [_P, _INT, _P]),
             ("lgo_ppr", None, [_P, _INT, _P, _INT, _INT, _D, _P]),
             ("lgo_wpr_forward", _INT, [_P, _INT, _P, _P, _D, _D, _INT, _P]),
@@ -173,6 +175,15 @@ class Oracle(_Base):
 
     def tc(self, level):
         return lgo().lgo_tc(self.h, level)
+
+    def avg_teen_cnt(self, level, age, K=0):
+        """(average, teen_cnt, sum, count) of task avg_teen_cnt."""
+        a = np.ascontiguousarray(age, dtype=np.int32)
+        out = np.zeros(self.V, np.int32)
+        S, c = _I64(), _I64()
+        avg = lgo().lgo_avg_teen_cnt(self.h, level, _p(a), int(K), _p(out), C.byref(S),
+                                     C.byref(c))
+        return avg, out, S.value, c.value
 
     def scc(self, level):
         out = np.empty(self.V, np.int64)

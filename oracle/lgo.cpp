@@ -347,6 +347,30 @@ void lgo_pagerank_pull(void* gp, int level, int max, double d, double* rank) {
 	} while (cnt < max);
 }
 
+// Average teen count: ll_b_avg_teen_cnt::run, avg_teen_cnt.h:96-139.  For
+// every vertex n, teen_cnt[n] = in-neighbours t with 10 <= age[t] < 20; over
+// the vertices with age[n] > K, sum the counts (int32 in the reference; here
+// int64, equal while the sum fits 31 bits) and return (float)(sum / count),
+// 0 when no vertex qualifies.
+double lgo_avg_teen_cnt(void* gp, int level, const int32_t* age, int K,
+		int32_t* teen_cnt, int64_t* sum_out, int64_t* cnt_out) {
+	Graph* g = (Graph*)gp;
+	std::vector<uint32_t> nb;
+	int64_t S = 0, cnt = 0;
+	for (uint64_t n = 0; n < g->V; n++) {
+		int32_t c = 0;
+		neighbours(g->in, level, n, nb, nullptr);
+		for (uint32_t t : nb)
+			if (age[t] >= 10 && age[t] < 20) c = c + 1;
+		teen_cnt[n] = c;
+		if (age[n] > K) { S += c; cnt += 1; }
+	}
+	*sum_out = S;
+	*cnt_out = cnt;
+	const double avg = (0 == cnt) ? 0.0 : ((double)S / (double)cnt);
+	return (double)(float)avg;
+}
+
 // BFS levels: u_sssp_bfs (sssp.h:219-244) / ll_b_sssp_unweighted_bfs::run
 // (sssp.h:285-300): dist = INT_MAX-1, dist[root] = 0, level-synchronous BFS
 // over out-edges.  Returns the number of reached vertices.

@@ -77,3 +77,28 @@ def test_scc_partition_exact(golden):
     O = build(golden)
     for l in range(len(golden["levels"])):
         assert np.array_equal(O.scc(l), golden[f"scc{l}"]), l
+
+
+def teen_expected(off, nbr, age, K):
+    """avg_teen_cnt from the reference's in-adjacency (its own iteration
+    order), as avg_teen_cnt.h:96-139 computes it."""
+    teen = (age >= 10) & (age < 20)
+    cs = np.concatenate([[0], np.cumsum(teen[nbr].astype(np.int64))])
+    o = off.astype(np.int64)
+    cnt = cs[o[1:]] - cs[o[:-1]]
+    sel = age > K
+    S, c = int(cnt[sel].sum()), int(sel.sum())
+    avg = float(np.float32(S / c)) if c else 0.0
+    return cnt.astype(np.int32), avg, S, c
+
+
+def test_avg_teen_cnt_matches_reference_adjacency(golden):
+    O = build(golden)
+    V = int(golden["V"])
+    rng = np.random.default_rng(21)
+    age = rng.integers(0, 60, V).astype(np.int32)
+    for l in range(len(golden["levels"])):
+        exp = teen_expected(golden[f"adj{l}_1_off"], golden[f"adj{l}_1_nbr"], age, 25)
+        avg, cnt, S, c = O.avg_teen_cnt(l, age, 25)
+        assert np.array_equal(cnt, exp[0]), l
+        assert (avg, S, c) == exp[1:], l
