@@ -174,6 +174,19 @@ lg_status lg_store_transfer_bytes(const lg_store* store, uint64_t* h2d,
  * LG_ESTATE while snapshots are open. */
 lg_status lg_store_drop_level(lg_store* store);
 
+/* Sliding window (the streaming mode's ll_mlcsr_ro_graph::set_min_level,
+ * llama/include/llama/ll_mlcsr_graph.h:560-602 and ll_mlcsr_sp.h:1810-1863,
+ * with LL_MIN_LEVEL): levels below min_level age out.  Their device arrays
+ * are freed, and every snapshot opened afterwards sees levels min_level..L
+ * only: a vertex's fragment chain ends at the first fragment of an older
+ * level, as iter_begin / iter_descend end it (ll_mlcsr_sp.h:2021-2026,
+ * 2107-2110).  Degrees in such a snapshot are the live edges inside the
+ * window.  min_level never decreases and must leave at least the newest level;
+ * LG_ESTATE while snapshots are open.  Deleting or re-adding an edge that
+ * lives only in aged-out levels sees it as not live. */
+lg_status lg_store_set_min_level(lg_store* store, int min_level);
+int       lg_store_min_level(const lg_store* store);
+
 /* Build the next level on the device from its edge delta instead of
  * ingesting a level the host built: the vertex tables and edge slots come out
  * as ll_mlcsr_core::init_level_from_degrees / init_node / write_values /
@@ -215,6 +228,13 @@ lg_status lg_store_read_level(lg_store* store, int level, int dir, lg_vt_entry* 
  * level = -1 selects the latest level.
  * ------------------------------------------------------------------------- */
 lg_status lg_snapshot_open(lg_store* store, int level, lg_snapshot** snap);
+/* A snapshot of `level` that sees levels min_level..level only (a sliding
+ * window; min_level >= lg_store_min_level).  lg_snapshot_open is this with
+ * the store's min level. */
+lg_status lg_snapshot_open_window(lg_store* store, int level, int min_level,
+		lg_snapshot** snap);
+/* Oldest level a snapshot sees. */
+lg_status lg_snapshot_min_level(const lg_snapshot* snap, int* min_level);
 lg_status lg_snapshot_close(lg_snapshot* snap);
 lg_status lg_snapshot_level(const lg_snapshot* snap, int* level);
 lg_status lg_snapshot_max_nodes(const lg_snapshot* snap, uint64_t* max_nodes);

@@ -135,6 +135,10 @@ SIGNATURES = [
     ("lg_store_read_level", _INT, [_P, _INT, _INT, _P, _P, _P, C.POINTER(_U64)]),
     ("lg_snapshot_get_stats", _INT, [_P, _INT, C.POINTER(lg_snapshot_stats)]),
     ("lg_snapshot_open", _INT, [_P, _INT, _PP]),
+    ("lg_snapshot_open_window", _INT, [_P, _INT, _INT, _PP]),
+    ("lg_snapshot_min_level", _INT, [_P, C.POINTER(_INT)]),
+    ("lg_store_set_min_level", _INT, [_P, _INT]),
+    ("lg_store_min_level", _INT, [_P]),
     ("lg_snapshot_close", _INT, [_P]),
     ("lg_snapshot_level", _INT, [_P, C.POINTER(_INT)]),
     ("lg_snapshot_max_nodes", _INT, [_P, C.POINTER(_U64)]),

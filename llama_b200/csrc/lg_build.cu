@@ -43,6 +43,7 @@ struct BuildTab {
 	const uint32_t* ids[LG_MAX_LEVELS];
 	const uint32_t* del[LG_MAX_LEVELS];
 	uint64_t max_nodes[LG_MAX_LEVELS];
+	int min_level;             // levels below are aged out (null above)
 };
 
 enum BuildErr : unsigned {
@@ -85,19 +86,21 @@ __global__ void bl_mark(const uint2* dels, uint64_t n, int L, BuildTab t) {
 	const uint2 d = dels[i];
 	const uint32_t lv = d.y >> LG_BITS_LEVEL;
 	const uint32_t ml = d.y & ((1u << LG_BITS_LEVEL) - 1u);
-	if ((int)lv > L || (int)ml > L) return;
+	if ((int)lv > L || (int)lv < t.min_level || (int)ml > L) return;
 	atomicOr(const_cast<uint32_t*>(t.del[lv]) + (d.x >> 5), 1u << (d.x & 31));
 }
 
 // Edge id of the slot holding (v -> x) live in snapshot `snap`, or -1: the
 // walk of iter_begin / iter_descend (ll_mlcsr_sp.h:1994-2134), each
-// fragment binary searched (fragments are sorted by neighbour id).
+// fragment binary searched (fragments are sorted by neighbour id), ending at
+// the aged-out levels.
 __device__ int64_t find_live(const BuildTab& t, int snap, uint32_t v, uint32_t x) {
 	if (v >= t.max_nodes[snap]) return -1;
 	lg_vt_entry e = t.vt[snap][v];
 	for (int step = 0; step < LG_MAX_LEVELS; step++) {
 		if (e.adj_list_start == LG_NIL_EDGE || e.level_length == 0) return -1;
 		const uint32_t lv = LG_EDGE_LEVEL(e.adj_list_start);
+		if ((int)lv < t.min_level) return -1;
 		const uint64_t idx = LG_EDGE_INDEX(e.adj_list_start);
 		const uint32_t* base = t.ids[lv] + idx;
 		uint32_t lo = 0, hi = e.level_length;
@@ -109,7 +112,7 @@ __device__ int64_t find_live(const BuildTab& t, int snap, uint32_t v, uint32_t x
 			const uint64_t k = idx + lo;
 			if (!((t.del[lv][k >> 5] >> (k & 31)) & 1u)) return (int64_t)LG_EDGE_CREATE(lv, k);
 		}
-		if (lv == 0 || v >= t.max_nodes[lv - 1]) return -1;
+		if ((int)lv <= t.min_level || v >= t.max_nodes[lv - 1]) return -1;
 		e = t.vt[lv - 1][v];
 	}
 	return -1;
@@ -231,14 +234,16 @@ static lg_status to_device(lg_store* s, const uint32_t* p, uint64_t n, DevBuf& b
 static lg_status build_tab(lg_store* s, const DevCsr& csr, DevBuf& bits, BuildTab* t) {
 	std::memset(t, 0, sizeof(*t));
 	const int L = (int)csr.levels.size() - 1;
+	const int m = s->min_level;
+	t->min_level = m;
 	if (L < 0) return LG_OK;
 	std::vector<uint64_t> word_off(L + 2, 0);
 	for (int l = 0; l <= L; l++)
-		word_off[l + 1] = word_off[l] + (csr.levels[l]->n_slots + 31) / 32 + 1;
-	LG_TRY(bits.reserve(word_off[L + 1] * sizeof(uint32_t)));
+		word_off[l + 1] = word_off[l] + (l < m ? 0 : (csr.levels[l]->n_slots + 31) / 32 + 1);
+	LG_TRY(bits.reserve(std::max<uint64_t>(word_off[L + 1], 1) * sizeof(uint32_t)));
 	LG_CUDA(cudaMemsetAsync(bits.p, 0, word_off[L + 1] * sizeof(uint32_t), s->stream),
 			"clear deletion bits");
-	for (int l = 0; l <= L; l++) {
+	for (int l = m; l <= L; l++) {
 		t->vt[l] = csr.levels[l]->vt.as<lg_vt_entry>();
 		t->ids[l] = csr.levels[l]->ids.as<uint32_t>();
 		t->del[l] = bits.as<uint32_t>() + word_off[l];
@@ -516,6 +521,7 @@ extern "C" lg_status lg_store_read_level(lg_store* s, int level, int dir, lg_vt_
 	if (level < 0 || level >= (int)csr.levels.size())
 		return set_error(LG_EINVAL, "level %d out of range", level);
 	const DevLevel* d = csr.levels[level];
+	if (level < s->min_level) return set_error(LG_ESTATE, "level %d is aged out", level);
 	if (weights && !d->w.p) return set_error(LG_ESTATE, "the level has no edge weights");
 	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
 	if (n_slots) *n_slots = d->n_slots;

@@ -229,6 +229,7 @@ struct lg_store {
 	lg::SnapDir* snap_spare[2] = {nullptr, nullptr};
 	lg::DevLevel* level_spare[2] = {nullptr, nullptr};
 	lg::DevBuf build_tmp[12];   // lg_store_build_level temporaries
+	int min_level = 0;          // levels below are aged out (lg_store_set_min_level)
 };
 
 // Edge-order maps of a snapshot used by the differentiable PageRank
@@ -241,6 +242,7 @@ struct lg_snapshot {
 	lg_adjoint_maps* adj_maps = nullptr;
 	lg::FlatCsr* flat[2] = {nullptr, nullptr};   // lg_snapshot_flatten, per direction
 	int level = 0;
+	int min_level = 0;          // oldest level the snapshot sees
 	uint64_t V = 0;
 	lg::SnapDir out, in;
 	lg::SnapCsr view(int dir) const {

@@ -172,7 +172,7 @@ lg_status build_flat(lg_snapshot* sn, int dir, FlatCsr& f, bool view) {
 	const unsigned B = 256;
 	const DevCsr& csr = dir == 0 ? s->out : s->in;
 	bool weighted = true;
-	for (int l = 0; l <= sn->level; l++)
+	for (int l = sn->min_level; l <= sn->level; l++)
 		if (csr.levels[l]->n_fragment_slots > 0 && !csr.levels[l]->w.p) weighted = false;
 
 	f.V = V;

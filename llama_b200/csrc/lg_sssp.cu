@@ -135,7 +135,7 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 		return set_error(LG_EINVAL, "root %lld out of range", (long long)root);
 	if (delta == 0) return set_error(LG_EINVAL, "delta must be positive");
 	lg_store* s = sn->store;
-	for (int l = 0; l <= sn->level; l++)
+	for (int l = sn->min_level; l <= sn->level; l++)
 		if (!s->out.levels[l]->w.p && s->out.levels[l]->n_fragment_slots > 0)
 			return set_error(LG_ESTATE, "level %d of the out-CSR carries no edge weights", l);
 	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");

@@ -383,8 +383,13 @@ struct VtTab {
 // by iter_descend is the element VT[level-1][v] copied when `level` was built
 // (ll_mlcsr_sp.h:1474-1497) and older levels never change afterwards, so the
 // walk reads that element directly.
+//
+// With a minimum level minL (the sliding window), the chain ends at the first
+// fragment of a level below minL, as iter_begin / iter_descend end it under
+// LL_MIN_LEVEL (ll_mlcsr_sp.h:2021-2026, 2107-2110); vertex tables of levels
+// below minL are never read.
 template <bool kFill>
-__global__ void walk_fragments(VtTab tab, int L, uint64_t V, uint32_t* count,
+__global__ void walk_fragments(VtTab tab, int L, int minL, uint64_t V, uint32_t* count,
 		uint32_t* deg, uint32_t* slots_per_vertex, const uint32_t* frag_off,
 		uint2* frags) {
 	uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -395,18 +400,22 @@ __global__ void walk_fragments(VtTab tab, int L, uint64_t V, uint32_t* count,
 	uint32_t out = kFill ? frag_off[v] : 0;
 	while (e.adj_list_start != LG_NIL_EDGE && e.level_length != 0) {
 		uint32_t lv = LG_EDGE_LEVEL(e.adj_list_start);
+		if ((int)lv < minL) break;
 		uint32_t ix = (uint32_t)LG_EDGE_INDEX(e.adj_list_start);
 		if (kFill) frags[out + n] = make_uint2(ix, (e.level_length << kLevelBits) | lv);
 		n++;
 		slots += e.level_length;
-		if (lv == 0 || v >= tab.max_nodes[lv - 1]) break;
+		if ((int)lv <= minL || v >= tab.max_nodes[lv - 1]) break;
 		e = tab.vt[lv - 1][v];
 	}
 	if (!kFill) { count[v] = n; slots_per_vertex[v] = slots; }
 }
 
+__global__ void live_counts(SnapCsr g, uint32_t* out);
+
 // Sets the bit of every slot deleted at or before L and counts them in *count.
-__global__ void mark_deletions(const uint2* dels, uint64_t n, int L,
+// Slots of levels below minL are outside the window and have no bitset.
+__global__ void mark_deletions(const uint2* dels, uint64_t n, int L, int minL,
 		uint32_t* const* del_words, unsigned long long* count) {
 	uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	bool hit = false;
@@ -414,7 +423,7 @@ __global__ void mark_deletions(const uint2* dels, uint64_t n, int L,
 		uint2 d = dels[i];
 		uint32_t lv = d.y >> LG_BITS_LEVEL;
 		uint32_t ml = d.y & ((1u << LG_BITS_LEVEL) - 1u);
-		if ((int)lv <= L && (int)ml <= L) {
+		if ((int)lv <= L && (int)lv >= minL && (int)ml <= L) {
 			atomicOr(del_words[lv] + (d.x >> 5), 1u << (d.x & 31));
 			hit = true;
 		}
@@ -452,11 +461,12 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 	const int L = sn->level;
 	SnapDir*& spare = s->snap_spare[&csr == &s->out ? 0 : 1];
 	if (spare) d.swap_buffers(*spare);       // a closed snapshot's device buffers
+	const int minL = sn->min_level;
 	const uint64_t V = csr.levels[L]->max_nodes;
 	cudaStream_t st = s->stream;
 	VtTab tab;
 	std::memset(&tab, 0, sizeof(tab));
-	for (int l = 0; l <= L; l++) {
+	for (int l = minL; l <= L; l++) {
 		tab.vt[l] = csr.levels[l]->vt.as<lg_vt_entry>();
 		tab.max_nodes[l] = csr.levels[l]->max_nodes;
 	}
@@ -468,7 +478,7 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 	LG_TRY(d.deg.reserve(V * sizeof(uint32_t)));
 	LG_TRY(d.frag_off.reserve((V + 1) * sizeof(uint32_t)));
 	const unsigned B = 256;
-	walk_fragments<false><<<grid_for(V, B), B, 0, st>>>(tab, L, V,
+	walk_fragments<false><<<grid_for(V, B), B, 0, st>>>(tab, L, minL, V,
 			cnt.as<uint32_t>(), d.deg.as<uint32_t>(), slots.as<uint32_t>(),
 			nullptr, nullptr);
 	LG_CUDA(cudaGetLastError(), "walk_fragments");
@@ -478,20 +488,21 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 			scan_tmp, st, &F));
 	d.n_frags = F;
 	LG_TRY(d.frags.reserve(std::max<uint64_t>(F, 1) * sizeof(uint2)));
-	walk_fragments<true><<<grid_for(V, B), B, 0, st>>>(tab, L, V, nullptr,
+	walk_fragments<true><<<grid_for(V, B), B, 0, st>>>(tab, L, minL, V, nullptr,
 			nullptr, nullptr, d.frag_off.as<uint32_t>(), d.frags.as<uint2>());
 	LG_CUDA(cudaGetLastError(), "walk_fragments fill");
 
-	// deletion bitsets of levels 0..L
+	// deletion bitsets of levels minL..L
 	std::vector<uint64_t> word_off(L + 2, 0);
 	for (int l = 0; l <= L; l++)
-		word_off[l + 1] = word_off[l] + (csr.levels[l]->n_slots + 31) / 32 + 1;
+		word_off[l + 1] = word_off[l]
+			+ (l < minL ? 0 : (csr.levels[l]->n_slots + 31) / 32 + 1);
 	LG_TRY(d.delbits.reserve(word_off[L + 1] * sizeof(uint32_t)));
 	LG_CUDA(cudaMemsetAsync(d.delbits.p, 0, word_off[L + 1] * sizeof(uint32_t), st),
 			"clear deletion bits");
 	LevelTab lt;
 	std::memset(&lt, 0, sizeof(lt));
-	for (int l = 0; l <= L; l++) {
+	for (int l = minL; l <= L; l++) {
 		lt.ids[l] = csr.levels[l]->ids.as<uint32_t>();
 		lt.del[l] = d.delbits.as<uint32_t>() + word_off[l];
 		lt.w[l] = csr.levels[l]->w.p ? csr.levels[l]->w.as<uint32_t>() : nullptr;
@@ -508,9 +519,22 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 		LG_CUDA(cudaMemcpyAsync(words.p, lt.del, sizeof(lt.del),
 				cudaMemcpyHostToDevice, st), "deletion table");
 		mark_deletions<<<grid_for(csr.n_dels_dev, B), B, 0, st>>>(
-				csr.dels.as<uint2>(), csr.n_dels_dev, L,
+				csr.dels.as<uint2>(), csr.n_dels_dev, L, minL,
 				(uint32_t* const*)words.p, counters.as<unsigned long long>() + 1);
 		LG_CUDA(cudaGetLastError(), "mark_deletions");
+		s->launches++;
+	}
+	if (minL > 0) {
+		// the vertex table's degree counts edges of every level: in a window
+		// the degree is the number of live slots the chain covers
+		SnapCsr g;
+		g.frag_off = d.frag_off.as<uint32_t>();
+		g.frags = d.frags.as<uint2>();
+		g.lt = d.lt.as<LevelTab>();
+		g.deg = d.deg.as<uint32_t>();
+		g.V = V;
+		live_counts<<<grid_for(V, B), B, 0, st>>>(g, d.deg.as<uint32_t>());
+		LG_CUDA(cudaGetLastError(), "window degrees");
 		s->launches++;
 	}
 
@@ -537,7 +561,7 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 	d.n_edges = sums[0];
 	d.n_frag_slots = total_slots;
 	d.n_slots = 0;
-	for (int l = 0; l <= L; l++) d.n_slots += csr.levels[l]->n_slots;
+	for (int l = minL; l <= L; l++) d.n_slots += csr.levels[l]->n_slots;
 	d.n_dels = sums[1];
 	d.present = true;
 	return LG_OK;
@@ -760,6 +784,8 @@ lg_status lg_store_drop_level(lg_store* s) {
 	if (s->out.levels.empty()) return set_error(LG_ESTATE, "the store holds no level");
 	if (s->open_snapshots > 0)
 		return set_error(LG_ESTATE, "close all snapshots before dropping a level");
+	if ((int)s->out.levels.size() - 1 <= s->min_level && s->min_level > 0)
+		return set_error(LG_ESTATE, "the newest level is the only one not aged out");
 	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
 	LG_CUDA(cudaStreamSynchronize(s->stream), "drop level");
 	for (int dir = 0; dir < 2; dir++) {
@@ -792,18 +818,23 @@ lg_status lg_snapshot_get_stats(const lg_snapshot* sn, int dir, lg_snapshot_stat
 	return LG_OK;
 }
 
-lg_status lg_snapshot_open(lg_store* s, int level, lg_snapshot** out) {
+lg_status lg_snapshot_open_window(lg_store* s, int level, int min_level,
+		lg_snapshot** out) {
 	clear_error();
 	if (!s || !out) return set_error(LG_EINVAL, "null argument");
 	*out = nullptr;
 	int n = (int)s->out.levels.size();
 	if (level < 0) level = n - 1;
 	if (level < 0 || level >= n) return set_error(LG_EINVAL, "no such level %d", level);
+	if (min_level < s->min_level || min_level > level)
+		return set_error(LG_EINVAL, "min_level %d outside [%d, %d] (levels below %d are "
+				"aged out)", min_level, s->min_level, level, s->min_level);
 	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
 	lg_snapshot* sn = new (std::nothrow) lg_snapshot();
 	if (!sn) return set_error(LG_ENOMEM, "host allocation");
 	sn->store = s;
 	sn->level = level;
+	sn->min_level = min_level;
 	sn->V = s->out.levels[level]->max_nodes;
 	lg_status st = open_dir(sn, s->out, sn->out);
 	if (!st && s->reverse) st = open_dir(sn, s->in, sn->in);
@@ -812,6 +843,47 @@ lg_status lg_snapshot_open(lg_store* s, int level, lg_snapshot** out) {
 	*out = sn;
 	return LG_OK;
 }
+
+lg_status lg_snapshot_open(lg_store* s, int level, lg_snapshot** out) {
+	if (!s) { clear_error(); return set_error(LG_EINVAL, "null argument"); }
+	int lv = level < 0 ? (int)s->out.levels.size() - 1 : level;
+	if (lv >= 0 && lv < s->min_level) {
+		clear_error();
+		return set_error(LG_EINVAL, "level %d is aged out (min level %d)", lv, s->min_level);
+	}
+	return lg_snapshot_open_window(s, level, s->min_level, out);
+}
+
+lg_status lg_snapshot_min_level(const lg_snapshot* sn, int* min_level) {
+	if (!sn || !min_level) return set_error(LG_EINVAL, "null argument");
+	*min_level = sn->min_level;
+	return LG_OK;
+}
+
+lg_status lg_store_set_min_level(lg_store* s, int m) {
+	clear_error();
+	if (!s) return set_error(LG_EINVAL, "null store");
+	const int n = (int)s->out.levels.size();
+	if (m < s->min_level) return set_error(LG_EINVAL, "the min level cannot decrease");
+	if (m > n - 1) return set_error(LG_EINVAL, "min level %d would age out every level", m);
+	if (s->open_snapshots > 0)
+		return set_error(LG_ESTATE, "close all snapshots before aging levels out");
+	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+	LG_CUDA(cudaStreamSynchronize(s->stream), "set min level");
+	for (int l = s->min_level; l < m; l++) {
+		for (DevCsr* c : {&s->out, &s->in}) {
+			if (l >= (int)c->levels.size()) continue;
+			DevLevel* d = c->levels[l];
+			d->vt.release();       // sizes (max_nodes, n_slots) stay for validation
+			d->ids.release();
+			d->w.release();
+		}
+	}
+	s->min_level = m;
+	return LG_OK;
+}
+
+int lg_store_min_level(const lg_store* s) { return s ? s->min_level : 0; }
 
 lg_status lg_snapshot_close(lg_snapshot* sn) {
 	clear_error();

@@ -218,8 +218,18 @@ class Store:
             return vt, ids, w[:n.value]
         return vt, ids
 
-    def snapshot(self, level=-1):
-        return Snapshot(self, level)
+    def snapshot(self, level=-1, min_level=None):
+        """Snapshot of `level`; with min_level, a sliding window over levels
+        min_level..level."""
+        return Snapshot(self, level, min_level)
+
+    @property
+    def min_level(self):
+        return lib.lg_store_min_level(self._h)
+
+    def set_min_level(self, m):
+        """Age out the levels below m (lg_store_set_min_level)."""
+        check(lib.lg_store_set_min_level(self._h, int(m)))
 
 
 class Tape:
@@ -264,16 +274,21 @@ def ppr(snapshots, seeds, iterations=20, damping=0.85, out=None):
 class Snapshot:
     """Read-only view of one level (``lg_snapshot``)."""
 
-    def __init__(self, store, level=-1):
+    def __init__(self, store, level=-1, min_level=None):
         h = C.c_void_p()
-        check(lib.lg_snapshot_open(store.handle, level, C.byref(h)))
+        if min_level is None:
+            check(lib.lg_snapshot_open(store.handle, level, C.byref(h)))
+        else:
+            check(lib.lg_snapshot_open_window(store.handle, level, int(min_level), C.byref(h)))
         self._h = h
         self.store = store
-        lv, mn = C.c_int(), C.c_uint64()
+        lv, mn, ml = C.c_int(), C.c_uint64(), C.c_int()
         check(lib.lg_snapshot_level(h, C.byref(lv)))
         check(lib.lg_snapshot_max_nodes(h, C.byref(mn)))
+        check(lib.lg_snapshot_min_level(h, C.byref(ml)))
         self.level = lv.value
         self.max_nodes = mn.value
+        self.min_level = ml.value
 
     def close(self):
         if self._h:

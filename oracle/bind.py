@@ -48,6 +48,7 @@ def lgo():
             ("lgo_bc", None, [_P, _INT, _P, _INT, _P]),
             ("lgo_sssp", _U64, [_P, _INT, _I64, _P]),
             ("lgo_tc", _I64, [_P, _INT]),
+            ("lgo_set_min_level", None, [_P, _INT]),
             ("lgo_avg_teen_cnt", _D, [_P, _INT, _P, _INT, _P, C.POINTER(_I64),
                                       C.POINTER(_I64)]),
             ("lgo_scc", None, [_P, _INT, _P]),
@@ -175,6 +176,10 @@ class Oracle(_Base):
 
     def tc(self, level):
         return lgo().lgo_tc(self.h, level)
+
+    def set_min_level(self, m):
+        """Sliding window: iteration ends at fragments of levels below m."""
+        lgo().lgo_set_min_level(self.h, int(m))
 
     def avg_teen_cnt(self, level, age, K=0):
         """(average, teen_cnt, sum, count) of task avg_teen_cnt."""

@@ -52,6 +52,7 @@ struct Csr {
 	std::vector<std::vector<VtEntry>> vt;     // per level, max_nodes + 1
 	std::vector<std::vector<uint64_t>> et;    // per level edge table
 	std::vector<std::vector<uint32_t>> w;     // per level edge property
+	uint64_t min_level = 0;                   // _minLevel, ll_mlcsr_sp.h:114-116
 };
 
 struct Iter {               // ll_edge_iterator, ll_mlcsr_iterator.h:53-68
@@ -74,6 +75,11 @@ void iter_descend(const Csr& c, Iter& it) {
 	VtEntry b;
 	memcpy(&b, &c.et[it.ptr_level][it.ptr_index + 1], sizeof(b));
 	it.edge = b.adj_list_start;
+	if (edge_level(it.edge) < c.min_level) {      // LL_MIN_LEVEL, :2107-2110
+		it.left = 0;
+		it.edge = NIL;
+		return;
+	}
 	it.left = b.level_length;
 	if (it.left == 0) it.edge = NIL;
 	else { it.ptr_level = edge_level(it.edge); it.ptr_index = edge_index(it.edge); }
@@ -110,6 +116,11 @@ void iter_begin(const Csr& c, Iter& it, int64_t n, int level) {
 	it.max_level = level;
 	const VtEntry& b = c.vt[level][n];
 	it.edge = b.adj_list_start;
+	if (edge_level(it.edge) < c.min_level) {      // LL_MIN_LEVEL, :2021-2026
+		it.left = 0;
+		it.edge = NIL;
+		return;
+	}
 	it.left = b.level_length;
 	if (it.left == 0) it.edge = NIL;
 	else { it.ptr_level = edge_level(it.edge); it.ptr_index = edge_index(it.edge); }
@@ -133,6 +144,21 @@ void neighbours(const Csr& c, int level, int64_t n, std::vector<uint32_t>& nb,
 		nb.push_back((uint32_t)it.last_node);
 		if (ids) ids->push_back(e);
 	}
+}
+
+// degree(n): the vertex-table degree (LL_PRECOMPUTED_DEGREE,
+// ll_mlcsr_sp.h:1900-1930).  In a sliding window it is the number of edges
+// the iterator yields: the reference leaves the windowed degree with
+// deletions unimplemented (ll_mlcsr_sp.h:1914-1928).
+std::vector<uint32_t> degrees_of(const Csr& c, int level, uint64_t V) {
+	std::vector<uint32_t> d(V);
+	std::vector<uint32_t> nb;
+	for (uint64_t v = 0; v < V; v++) {
+		if (c.min_level == 0) { d[v] = c.vt[level][v].degree; continue; }
+		neighbours(c, level, (int64_t)v, nb, nullptr);
+		d[v] = (uint32_t)nb.size();
+	}
+	return d;
 }
 
 // find, ll_mlcsr_sp.h:2334-2356: first edge of n whose payload is `value`.
@@ -236,6 +262,14 @@ void lgo_destroy(void* g) { delete (Graph*)g; }
 
 int lgo_num_levels(void* gp) { return (int)((Graph*)gp)->out.vt.size(); }
 
+// Sliding window: ll_mlcsr_ro_graph::set_min_level (ll_mlcsr_graph.h:560-602)
+// on both CSRs.
+void lgo_set_min_level(void* gp, int m) {
+	Graph* g = (Graph*)gp;
+	g->out.min_level = (uint64_t)m;
+	g->in.min_level = (uint64_t)m;
+}
+
 // Append a level: new edges (any order), deleted edges (live in the latest
 // snapshot), optional weights per new edge.  Deletions lower the slot's
 // max_visible_level to the new level number in both CSRs
@@ -322,7 +356,8 @@ uint64_t lgo_adjacency(void* gp, int dir, int level, uint64_t* offsets,
 void lgo_degrees(void* gp, int dir, int level, uint32_t* deg) {
 	Graph* g = (Graph*)gp;
 	Csr& c = dir == 0 ? g->out : g->in;
-	for (uint64_t v = 0; v < g->V; v++) deg[v] = c.vt[level][v].degree;
+	std::vector<uint32_t> d = degrees_of(c, level, g->V);
+	for (uint64_t v = 0; v < g->V; v++) deg[v] = d[v];
 }
 
 // PageRank pull, FP64: ll_b_pagerank_pull_ext::run, pagerank.h:98-182.
@@ -333,13 +368,14 @@ void lgo_pagerank_pull(void* gp, int level, int max, double d, double* rank) {
 	std::vector<double> nxt(V);
 	for (uint64_t t = 0; t < V; t++) rank[t] = 1 / N;
 	std::vector<uint32_t> nb;
+	const std::vector<uint32_t> od = degrees_of(g->out, level, V);
 	int cnt = 0;
 	do {
 		for (uint64_t t = 0; t < V; t++) {
 			double S = 0.0;
 			neighbours(g->in, level, t, nb, nullptr);
 			for (uint32_t w : nb)
-				S = S + rank[w] / ((double)g->out.vt[level][w].degree);
+				S = S + rank[w] / ((double)od[w]);
 			nxt[t] = (1 - d) / N + d * S;
 		}
 		for (uint64_t t = 0; t < V; t++) rank[t] = nxt[t];
@@ -642,6 +678,7 @@ void lgo_ppr(void* gp, int level, const int64_t* seeds, int K, int iters,
 	std::vector<uint32_t> nb;
 	std::vector<std::vector<uint32_t>> in(V);
 	for (uint64_t t = 0; t < V; t++) neighbours(g->in, level, t, in[t], nullptr);
+	const std::vector<uint32_t> od = degrees_of(g->out, level, V);
 	for (int k = 0; k < K; k++) {
 		std::fill(x.begin(), x.end(), 0.0);
 		x[seeds[k]] = 1.0;
@@ -649,7 +686,7 @@ void lgo_ppr(void* gp, int level, const int64_t* seeds, int K, int iters,
 			for (uint64_t t = 0; t < V; t++) {
 				double S = 0.0;
 				for (uint32_t w : in[t])
-					S = S + x[w] / ((double)g->out.vt[level][w].degree);
+					S = S + x[w] / ((double)od[w]);
 				nx[t] = ((int64_t)t == seeds[k] ? (1 - d) : 0.0) + d * S;
 			}
 			x.swap(nx);

@@ -102,3 +102,30 @@ def test_avg_teen_cnt_matches_reference_adjacency(golden):
         avg, cnt, S, c = O.avg_teen_cnt(l, age, 25)
         assert np.array_equal(cnt, exp[0]), l
         assert (avg, S, c) == exp[1:], l
+
+
+def window_filter(off, nbr, ids, m):
+    """Adjacency of a sliding window over levels >= m: the chain ends at the
+    first fragment below m, and fragment levels fall along the chain, so this
+    is the full iteration restricted to edges whose level is >= m."""
+    keep = (ids.astype(np.uint64) >> np.uint64(38)) >= m
+    o = off.astype(np.int64)
+    cs = np.concatenate([[0], np.cumsum(keep.astype(np.int64))])
+    cnt = cs[o[1:]] - cs[o[:-1]]
+    return np.concatenate([[0], np.cumsum(cnt)]).astype(np.uint64), nbr[keep], cnt
+
+
+def test_oracle_window_matches_filtered_reference_iteration(golden):
+    for l in range(1, len(golden["levels"])):
+        full = build(golden)
+        for m in range(1, l + 1):
+            O = build(golden)
+            O.set_min_level(m)
+            for dr in (0, 1):
+                off, nb, ids = full.adjacency(l, dr)
+                assert np.array_equal(off, golden[f"adj{l}_{dr}_off"])
+                eo, en, ecnt = window_filter(off, nb, ids, m)
+                wo, wn, _ = O.adjacency(l, dr)
+                assert np.array_equal(wo, eo) and np.array_equal(wn, en), (l, m, dr)
+                if dr == 0:
+                    assert np.array_equal(O.degrees(l, 0), ecnt.astype(np.uint32))
