@@ -13,12 +13,13 @@
 // atomicMin on 32-bit distances, so the result does not depend on thread
 // order.  Per-vertex stamps keep every vertex at most once in the near queue
 // of a round and at most once in the far pile, which bounds both by V.
-#include "lg_device.cuh"
+#include "lg_expand.cuh"
 
 namespace lg {
 
 constexpr uint32_t kInf = LG_UNREACHED;
 constexpr int kSsspThreads = 256;
+constexpr uint32_t kSsspRange = 1024;     // slots per warp range
 
 __global__ void sssp_init(uint32_t* dist, uint32_t* stamp, uint32_t* fstamp,
 		uint64_t V, uint32_t root, uint32_t* queue) {
@@ -43,40 +44,41 @@ __device__ __forceinline__ void warp_push(bool take, uint32_t item,
 	if (take) queue[base + __popc(m & ((1u << lane) - 1u))] = item;
 }
 
-// ctr[0] near-next length, ctr[1] far length (starts at the current pile
-// size), ctr[2] relaxations
+// One relaxation round over the near queue.  The queue's slot space
+// (pos = exclusive prefix of the queued vertices' slot counts, pos[qlen] the
+// total, both written earlier on the stream) is cut into kSsspRange-slot
+// ranges that the grid's warps take in turn, so a hub in the queue is spread
+// over many warps.  ctr[0] near-next length, ctr[1] far length (starts at
+// the current pile size), ctr[2] relaxations.
 __global__ void __launch_bounds__(kSsspThreads)
-sssp_relax(SnapCsr out, const uint32_t* queue, uint32_t qlen, uint32_t* dist,
-		uint32_t* stamp, uint32_t* fstamp, uint32_t round, uint32_t epoch,
+sssp_relax(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
+		uint32_t* dist, uint32_t* stamp, uint32_t* fstamp, uint32_t round, uint32_t epoch,
 		uint32_t hi, uint32_t* near_next, uint32_t* far, unsigned long long* ctr) {
 	const uint32_t lane = threadIdx.x & 31u;
-	const uint64_t i = ((uint64_t)blockIdx.x * (kSsspThreads / 32) + (threadIdx.x >> 5)) * 32 + lane;
-	const bool valid = i < qlen;
-	uint32_t cnt = 0, f0 = 0, du = 0;
-	if (valid) {
-		const uint32_t u = __ldg(queue + i);
-		du = __ldcg(dist + u);
-		cnt = vertex_slots(out, u, &f0);
-	}
+	const uint32_t total = __ldg(pos + qlen);
+	const uint32_t nranges = (total + kSsspRange - 1) / kSsspRange;
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
 	unsigned long long relax = 0;
-	warp_expand(out, cnt, f0,
-		[&](bool act, uint32_t o, uint32_t nbr, uint32_t lv, uint32_t idx) {
-			const uint32_t dsrc = __shfl_sync(0xffffffffu, du, o);
-			bool to_near = false, to_far = false;
-			if (act) {
-				const uint32_t nd = dsrc + __ldg(out.lt->w[lv] + idx);
-				if (nd < __ldcg(dist + nbr)) {
-					const uint32_t old = atomicMin(dist + nbr, nd);
-					relax++;
-					if (nd < old) {
-						if (nd < hi) to_near = atomicExch(stamp + nbr, round) != round;
-						else to_far = atomicExch(fstamp + nbr, epoch) != epoch;
+	for (uint32_t r = warp; r < nranges; r += nwarps) {
+		range_for_each(out, queue, pos, qlen, total, nranges, kSsspRange, r,
+			[&](bool act, uint32_t, uint32_t ov, uint32_t nbr, uint32_t lv, uint32_t idx) {
+				bool to_near = false, to_far = false;
+				if (act) {
+					const uint32_t nd = __ldcg(dist + ov) + __ldg(out.lt->w[lv] + idx);
+					if (nd < __ldcg(dist + nbr)) {
+						const uint32_t old = atomicMin(dist + nbr, nd);
+						relax++;
+						if (nd < old) {
+							if (nd < hi) to_near = atomicExch(stamp + nbr, round) != round;
+							else to_far = atomicExch(fstamp + nbr, epoch) != epoch;
+						}
 					}
 				}
-			}
-			warp_push(to_near, nbr, near_next, ctr);
-			warp_push(to_far, nbr, far, ctr + 1);
-		});
+				warp_push(to_near, nbr, near_next, ctr);
+				warp_push(to_far, nbr, far, ctr + 1);
+			});
+	}
 	for (int o = 16; o > 0; o >>= 1) relax += __shfl_down_sync(0xffffffffu, relax, o);
 	if (lane == 0 && relax) atomicAdd(ctr + 2, relax);
 }
@@ -148,6 +150,12 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 	LG_TRY(sc[3].reserve(V * 4));          // far pile being compacted
 	LG_TRY(sc[5].reserve(2 * V * 4));      // near and far stamps
 	LG_TRY(sc[6].reserve(8 * sizeof(unsigned long long)));
+	LG_TRY(sc[7].reserve((2 * V + 1) * 4));   // queue slot counts and their prefix
+	uint32_t* qcnt = sc[7].as<uint32_t>();
+	uint32_t* qpos = qcnt + V;
+	int sms = 148;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+	const unsigned relax_blocks = (unsigned)sms * 8u;   // persistent over the ranges
 	const bool dev_out = is_device_pointer(dist);
 	uint32_t* d = dist;
 	if (!dev_out) { LG_TRY(sc[4].reserve(V * 4)); d = sc[4].as<uint32_t>(); }
@@ -203,11 +211,12 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 		unsigned long long init[3] = {0, flen, 0};
 		LG_CUDA(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st), "h2d");
 		s->h2d_bytes += sizeof(init);
-		uint64_t warps = (qlen + 31) / 32;
-		sssp_relax<<<grid_for(warps, kSsspThreads / 32), kSsspThreads, 0, st>>>(
-				out, q, (uint32_t)qlen, d, stamp, fstamp, round, epoch, hi, qn, far, ctr);
+		list_slots<<<grid_for(qlen, 256), 256, 0, st>>>(out, q, (uint32_t)qlen, qcnt);
+		LG_TRY(exclusive_scan_u32(qcnt, qpos, qlen, sc[8], st, nullptr));
+		sssp_relax<<<relax_blocks, kSsspThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, d,
+				stamp, fstamp, round, epoch, hi, qn, far, ctr);
 		LG_CUDA(cudaGetLastError(), "sssp_relax");
-		s->launches++;
+		s->launches += 5;
 		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
 		LG_CUDA(cudaStreamSynchronize(st), "sssp relax");
 		s->d2h_bytes += sizeof(h);
