@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--levels", type=int, default=8)
     p.add_argument("--pr-iters", type=int, default=20)
     p.add_argument("--roots", type=int, default=16)
+    p.add_argument("--bfs", default="multi", choices=["multi", "single"],
+                   help="BFS from all roots in one lg_bfs_multi call, or one lg_bfs per root")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-extras", action="store_true",
@@ -67,6 +69,9 @@ def workload(args):
                     f"{args.levels} levels (90% in level 0, 0.2% deletions per level)",
            "step": f"flatten the in-CSR + PageRank pull FP64 x{args.pr_iters} iterations "
                    f"+ BFS from {args.roots} roots, latest snapshot",
+           "bfs_mode": ("all roots in one multi-source call (lg_bfs_multi, 64 roots per "
+                        "bit-parallel pass; each row equals a single-root BFS)"
+                        if args.bfs == "multi" else "one lg_bfs call per root"),
            "pr_iterations": args.pr_iters, "damping": 0.85, "bfs_roots": args.roots}
     return spec, cfg
 
@@ -251,9 +256,13 @@ def run_lg(args):
         sn.pagerank_pull(args.pr_iters, 0.85, out=pr_dev)
         ev[1].record(stream)
         reach = 0
-        for i, r in enumerate(roots):
-            _, res = sn.bfs(int(r), out=lv_dev[i])
-            reach += res.reach_edges
+        if args.bfs == "multi":
+            _, rs = sn.bfs_multi(roots, out=lv_dev)
+            reach = sum(r.reach_edges for r in rs)
+        else:
+            for i, r in enumerate(roots):
+                _, res = sn.bfs(int(r), out=lv_dev[i])
+                reach += res.reach_edges
         ev[2].record(stream)
         sn.unflatten()
         return reach
@@ -407,9 +416,13 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
         if phase:
             phase("flatten_pagerank_to_host")
         reach = 0
-        for i, r in enumerate(roots):
-            _, res = s2.bfs(int(r), out=lv_host[i])
-            reach += res.reach_edges
+        if args.bfs == "multi":
+            _, rs = s2.bfs_multi(roots, out=lv_host)
+            reach = sum(r.reach_edges for r in rs)
+        else:
+            for i, r in enumerate(roots):
+                _, res = s2.bfs(int(r), out=lv_host[i])
+                reach += res.reach_edges
         if phase:
             phase("bfs_to_host")
         s2.close()

@@ -344,6 +344,18 @@ typedef struct lg_bfs_result {
 lg_status lg_bfs(lg_snapshot* snap, int64_t root, int32_t* levels,
 		lg_bfs_result* result);
 
+/* BFS levels from n_roots roots in one call: the same arrays as n_roots
+ * calls of lg_bfs (BFS levels are unique).  The roots share their
+ * traversals 64 at a time: every vertex carries one bit per root
+ * (bit-parallel multi-source BFS), so an edge visit serves every root whose
+ * frontier crosses it at that depth.  levels: int32[n_roots][max_nodes] (row
+ * k for roots[k]); results: lg_bfs_result[n_roots] or NULL (top_down_steps /
+ * bottom_up_steps count the shared steps of the root's group of 64).  Uses
+ * the snapshot's flat CSRs when lg_snapshot_flatten made them.  No reference
+ * counterpart as a single call; each row equals task sssp_unweighted. */
+lg_status lg_bfs_multi(lg_snapshot* snap, const int64_t* roots, int n_roots,
+		int32_t* levels, lg_bfs_result* results);
+
 /* Weighted single-source shortest paths: task "sssp_weighted",
  * ll_b_sssp_weighted::run (benchmark/benchmarks/sssp.h:97-183), whose
  * frontier Bellman-Ford reads G_len[e], the per-slot edge property

@@ -6,7 +6,7 @@
 // dist[root] = 0, unreached vertices keep INT_MAX - 1.  BFS levels are
 // unique, so any level-synchronous traversal yields the same array; this one
 // is direction-optimising (Beamer et al., SC'12): top-down steps expand the
-// frontier queue over the out-CSR with warp_expand, bottom-up steps let every
+// frontier queue over the out-CSR in balanced slot ranges, bottom-up steps let every
 // unvisited vertex look for a parent among its in-neighbours (in-CSR) in a
 // frontier bitmap that stays resident in L2.
 #include "lg_expand.cuh"

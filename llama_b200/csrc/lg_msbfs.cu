@@ -1,0 +1,390 @@
+// lg_msbfs.cu - BFS levels from many roots at once.
+//
+// Reference: the same task as lg_bfs (u_sssp_bfs / ll_b_sssp_unweighted_bfs,
+// benchmark/benchmarks/sssp.h:219-300), run for every root: dist[root] = 0,
+// level-synchronous, unreached vertices keep INT_MAX - 1.  The benchmark
+// runs one BFS per root; since BFS levels are unique, the roots can share
+// their traversals: every vertex carries a 64-bit mask per pass, one bit per
+// root (bit-parallel multi-source BFS), so one edge visit serves up to 64
+// BFSs whose frontiers cross it in the same step.
+//
+//   seen[v]   roots that reached v
+//   cur[v]    roots whose frontier holds v at the current depth
+//   nxt[v]    roots that reach v at the next depth (candidates)
+//
+// A step is top-down over the union frontier queue (out-CSR, balanced
+// 1024-slot ranges: nxt[w] |= cur[u] & ~seen[w]) or bottom-up (every vertex
+// some root has not reached ORs cur[] over its in-neighbours until every
+// missing root is found; flat in-CSR when the snapshot has one).  A commit
+// pass turns nxt into the new frontier, sets seen, and writes depth + 1 into
+// the level arrays of the new roots' bits.
+#include "lg_expand.cuh"
+#include "lg_flat.cuh"
+
+namespace lg {
+
+typedef unsigned long long u64;
+constexpr int32_t kMsUnreached = LG_UNREACHED;
+constexpr int kMsThreads = 256;
+constexpr uint32_t kMsRange = 1024;
+constexpr int kMsChunk = 4;            // in-neighbours per bottom-up round
+constexpr int kMsMaxRoots = 64;        // roots per pass
+
+__global__ void ms_fill(int32_t* levels, uint64_t n) {
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+			i += (uint64_t)gridDim.x * blockDim.x)
+		levels[i] = kMsUnreached;
+}
+
+// Roots k of this pass: bit k of seen and cur, level 0, the root queue.
+// ctr[0] queue length, ctr[1] out-degree sum of the queued roots.
+__global__ void ms_roots(const int64_t* roots, int n, uint64_t V, const uint32_t* outdeg,
+		u64* seen, u64* cur, int32_t* levels, uint32_t* queue, unsigned long long* ctr) {
+	const int k = threadIdx.x;
+	if (k >= n) return;
+	const uint32_t v = (uint32_t)roots[k];
+	atomicOr(seen + v, 1ull << k);
+	const u64 old = atomicOr(cur + v, 1ull << k);
+	levels[(uint64_t)k * V + v] = 0;
+	// the first root to mark v queues it (duplicates share the entry)
+	if (old == 0) {
+		queue[atomicAdd(ctr, 1ull)] = v;
+		atomicAdd(ctr + 1, (unsigned long long)__ldg(outdeg + v));
+	}
+}
+
+__device__ __forceinline__ void ms_push(bool take, uint32_t item, uint32_t* queue,
+		unsigned long long* len) {
+	const unsigned m = __ballot_sync(0xffffffffu, take);
+	if (!m) return;
+	const uint32_t lane = threadIdx.x & 31u;
+	const int leader = __ffs(m) - 1;
+	unsigned long long base = 0;
+	if ((int)lane == leader) base = atomicAdd(len, (unsigned long long)__popc(m));
+	base = __shfl_sync(0xffffffffu, base, leader);
+	if (take) queue[base + __popc(m & ((1u << lane) - 1u))] = item;
+}
+
+// Top-down: queue = union frontier, pos its slot prefix (pos[qlen] total);
+// a candidate w goes to `cand` the first time its nxt turns non-zero.
+__global__ void __launch_bounds__(kMsThreads)
+ms_top_down(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
+		const u64* cur, const u64* seen, u64* nxt, uint32_t* cand, unsigned long long* ncand) {
+	const uint32_t total = __ldg(pos + qlen);
+	const uint32_t nranges = (total + kMsRange - 1) / kMsRange;
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (uint32_t r = warp; r < nranges; r += nwarps) {
+		range_for_each(out, queue, pos, qlen, total, nranges, kMsRange, r,
+			[&](bool act, uint32_t, uint32_t ov, uint32_t nbr, uint32_t, uint32_t) {
+				bool first = false;
+				if (act) {
+					const u64 bits = __ldg(cur + ov) & ~__ldcg(seen + nbr);
+					if (bits && (__ldcg(nxt + nbr) & bits) != bits)
+						first = atomicOr(nxt + nbr, bits) == 0;
+				}
+				ms_push(first, nbr, cand, ncand);
+			});
+	}
+}
+
+// Bottom-up over a flat in-CSR: a thread takes kBuVerts vertices (blockDim
+// apart) and ORs cur[] over kMsChunk in-neighbours of each per round until
+// every root that has not reached the vertex is found, or the list ends.
+constexpr int kMsVerts = 4;
+__global__ void __launch_bounds__(kMsThreads)
+ms_bottom_up_flat(const uint32_t* off, const uint32_t* ids, uint32_t V, u64 lanes,
+		const u64* cur, const u64* seen, u64* nxt) {
+	const uint32_t base = blockIdx.x * (uint32_t)(kMsThreads * kMsVerts) + threadIdx.x;
+	uint32_t k[kMsVerts], end[kMsVerts];
+	u64 need[kMsVerts], got[kMsVerts];
+#pragma unroll
+	for (int j = 0; j < kMsVerts; j++) {
+		const uint32_t v = base + j * kMsThreads;
+		k[j] = 0; end[j] = 0; need[j] = 0; got[j] = 0;
+		if (v < V) {
+			need[j] = lanes & ~seen[v];
+			if (need[j]) { k[j] = __ldg(off + v); end[j] = __ldg(off + v + 1); }
+		}
+	}
+	bool more = true;
+	while (more) {
+		uint32_t u[kMsVerts][kMsChunk];
+#pragma unroll
+		for (int j = 0; j < kMsVerts; j++)
+#pragma unroll
+			for (int c = 0; c < kMsChunk; c++)
+				u[j][c] = k[j] + c < end[j] ? __ldg(ids + k[j] + c) : kNoId;
+		u64 f[kMsVerts][kMsChunk];
+#pragma unroll
+		for (int j = 0; j < kMsVerts; j++)
+#pragma unroll
+			for (int c = 0; c < kMsChunk; c++)
+				f[j][c] = u[j][c] != kNoId ? __ldg(cur + u[j][c]) : 0ull;
+		more = false;
+#pragma unroll
+		for (int j = 0; j < kMsVerts; j++) {
+#pragma unroll
+			for (int c = 0; c < kMsChunk; c++) got[j] |= f[j][c];
+			if ((got[j] & need[j]) == need[j]) k[j] = end[j];
+			else k[j] = min(k[j] + kMsChunk, end[j]);
+			more |= k[j] < end[j];
+		}
+	}
+#pragma unroll
+	for (int j = 0; j < kMsVerts; j++) {
+		const uint32_t v = base + j * kMsThreads;
+		const u64 b = got[j] & need[j];
+		if (b) nxt[v] = b;
+	}
+}
+
+// Bottom-up over the snapshot's fragments (no flat in-CSR): a thread per
+// vertex walks its fragments, skipping deleted slots.
+__global__ void __launch_bounds__(kMsThreads)
+ms_bottom_up(SnapCsr in, u64 lanes, const u64* cur, const u64* seen, u64* nxt) {
+	const uint64_t v64 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (v64 >= in.V) return;
+	const uint32_t v = (uint32_t)v64;
+	const u64 need = lanes & ~seen[v];
+	if (!need) return;
+	u64 got = 0;
+	const uint32_t f0 = __ldg(in.frag_off + v), f1 = __ldg(in.frag_off + v + 1);
+	for (uint32_t f = f0; f < f1 && (got & need) != need; f++) {
+		const uint2 fr = in.frags[f];
+		const uint32_t lv = frag_level(fr), n = frag_len(fr);
+		const uint32_t* ids = in.lt->ids[lv] + fr.x;
+		for (uint32_t k = 0; k < n && (got & need) != need; k++) {
+			if (slot_deleted(in.lt, lv, fr.x + k)) continue;
+			got |= __ldg(cur + __ldg(ids + k));
+		}
+	}
+	if (got & need) nxt[v] = got & need;
+}
+
+// Commit candidates (list, or every vertex when list is null): new roots'
+// bits become the next frontier (cur2, zero before), are added to seen and
+// get level depth + 1; the vertex joins the next queue.  ctr[0] next queue
+// length, ctr[1] its out-degree sum, ctr[2] OR of the new bits.
+__global__ void ms_commit(const uint32_t* list, uint32_t n, uint32_t depth1, uint64_t V,
+		u64* nxt, u64* seen, u64* cur2, int32_t* levels, const uint32_t* outdeg,
+		uint32_t* queue, unsigned long long* ctr) {
+	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	uint32_t w = 0;
+	u64 bits = 0;
+	if (i < n) {
+		w = list ? __ldg(list + i) : (uint32_t)i;
+		const u64 c = nxt[w];
+		if (c) {
+			nxt[w] = 0;
+			bits = c & ~seen[w];
+			if (bits) {
+				seen[w] |= bits;
+				cur2[w] = bits;
+				for (u64 b = bits; b; b &= b - 1)
+					levels[(uint64_t)(__ffsll((long long)b) - 1) * V + w] = (int32_t)depth1;
+			}
+		}
+	}
+	ms_push(bits != 0, w, queue, ctr);
+	unsigned long long e = bits ? __ldg(outdeg + w) : 0ull;
+	u64 any = bits;
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		e += __shfl_xor_sync(0xffffffffu, e, o);
+		any |= __shfl_xor_sync(0xffffffffu, any, o);
+	}
+	if ((threadIdx.x & 31u) == 0) {
+		if (e) atomicAdd(ctr + 1, e);
+		if (any) atomicOr(ctr + 2, any);
+	}
+}
+
+__global__ void ms_clear(const uint32_t* queue, uint32_t n, u64* cur) {
+	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) cur[__ldg(queue + i)] = 0;
+}
+
+// Per-root reached vertices and the out-degree sum over them.
+__global__ void ms_reach(const u64* seen, const uint32_t* outdeg, uint64_t V, int n,
+		unsigned long long* cnt, unsigned long long* edges) {
+	__shared__ unsigned long long sc[kMsMaxRoots], se[kMsMaxRoots];
+	for (int k = threadIdx.x; k < kMsMaxRoots; k += blockDim.x) { sc[k] = 0; se[k] = 0; }
+	__syncthreads();
+	for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V;
+			v += (uint64_t)gridDim.x * blockDim.x) {
+		u64 b = seen[v];
+		if (!b) continue;
+		const unsigned long long d = __ldg(outdeg + v);
+		for (; b; b &= b - 1) {
+			const int k = __ffsll((long long)b) - 1;
+			atomicAdd(sc + k, 1ull);
+			atomicAdd(se + k, d);
+		}
+	}
+	__syncthreads();
+	for (int k = threadIdx.x; k < n; k += blockDim.x) {
+		if (sc[k]) atomicAdd(cnt + k, sc[k]);
+		if (se[k]) atomicAdd(edges + k, se[k]);
+	}
+}
+
+} // namespace lg
+
+using namespace lg;
+
+extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_roots,
+		int32_t* levels, lg_bfs_result* results) {
+	clear_error();
+	if (!sn || !roots || !levels) return set_error(LG_EINVAL, "null argument");
+	if (n_roots <= 0) return set_error(LG_EINVAL, "n_roots must be positive");
+	for (int k = 0; k < n_roots; k++)
+		if (roots[k] < 0 || (uint64_t)roots[k] >= sn->V)
+			return set_error(LG_EINVAL, "root %lld out of range", (long long)roots[k]);
+	lg_store* s = sn->store;
+	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+	cudaStream_t st = s->stream;
+	const uint64_t V = sn->V;
+	const unsigned B = 256;
+	DevBuf* sc = s->scratch;
+	LG_TRY(sc[0].reserve(2 * V * sizeof(u64)));            // seen, nxt
+	LG_TRY(sc[1].reserve(2 * V * sizeof(u64)));            // cur, cur2
+	LG_TRY(sc[2].reserve(2 * V * sizeof(uint32_t)));       // queue, next queue
+	LG_TRY(sc[3].reserve(V * sizeof(uint32_t)));           // candidates
+	LG_TRY(sc[5].reserve((2 * V + 1) * sizeof(uint32_t))); // slot counts, prefix
+	LG_TRY(sc[6].reserve((8 + 2 * kMsMaxRoots) * sizeof(unsigned long long)));
+	u64* seen = sc[0].as<u64>();
+	u64* nxt = seen + V;
+	u64* cur = sc[1].as<u64>();
+	u64* cur2 = cur + V;
+	uint32_t* q = sc[2].as<uint32_t>();
+	uint32_t* q2 = q + V;
+	uint32_t* cand = sc[3].as<uint32_t>();
+	uint32_t* qcnt = sc[5].as<uint32_t>();
+	uint32_t* qpos = qcnt + V;
+	unsigned long long* ctr = sc[6].as<unsigned long long>();
+	unsigned long long* lane_cnt = ctr + 8;
+	unsigned long long* lane_edges = lane_cnt + kMsMaxRoots;
+	const bool dev_out = is_device_pointer(levels);
+	int32_t* lv = levels;
+	if (!dev_out) {
+		LG_TRY(sc[4].reserve((uint64_t)n_roots * V * sizeof(int32_t)));
+		lv = sc[4].as<int32_t>();
+	}
+	// flat views where lg_snapshot_flatten made them
+	const FlatCsr* fo = sn->flat[0];
+	const FlatCsr* fi = sn->flat[1];
+	const SnapCsr out = (fo && fo->has_view) ? fo->view(sn->out.deg.as<uint32_t>()) : sn->view(0);
+	const bool has_in = sn->in.present;
+	const SnapCsr in = has_in ? sn->view(1) : out;
+	const uint32_t* outdeg = sn->out.deg.as<uint32_t>();
+	int sms = 148;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+	const unsigned td_blocks = (unsigned)sms * 8u;
+	const double alpha = 14.0, beta = 24.0;
+
+	ms_fill<<<(unsigned)sms * 16u, B, 0, st>>>(lv, (uint64_t)n_roots * V);
+	LG_CUDA(cudaGetLastError(), "ms_fill");
+	s->launches++;
+	for (int p0 = 0; p0 < n_roots; p0 += kMsMaxRoots) {
+		const int n = std::min(kMsMaxRoots, n_roots - p0);
+		const u64 lanes = n == 64 ? ~0ull : ((1ull << n) - 1ull);
+		int32_t* plv = lv + (uint64_t)p0 * V;
+		// (the previous pass swapped the pairs)
+		cur = sc[1].as<u64>();
+		cur2 = cur + V;
+		q = sc[2].as<uint32_t>();
+		q2 = q + V;
+		LG_CUDA(cudaMemsetAsync(seen, 0, 2 * V * sizeof(u64), st), "clear masks");
+		LG_CUDA(cudaMemsetAsync(cur, 0, 2 * V * sizeof(u64), st), "clear masks");
+		LG_CUDA(cudaMemsetAsync(ctr, 0, (8 + 2 * kMsMaxRoots) * sizeof(unsigned long long), st),
+				"clear counters");
+		LG_TRY(sc[7].reserve(kMsMaxRoots * sizeof(int64_t)));
+		LG_CUDA(cudaMemcpyAsync(sc[7].p, roots + p0, n * sizeof(int64_t),
+				cudaMemcpyHostToDevice, st), "roots");
+		s->h2d_bytes += n * sizeof(int64_t);
+		ms_roots<<<1, kMsMaxRoots, 0, st>>>(sc[7].as<int64_t>(), n, V, outdeg, seen, cur, plv,
+				q, ctr);
+		LG_CUDA(cudaGetLastError(), "ms_roots");
+		s->launches++;
+		unsigned long long h[3];
+		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+		LG_CUDA(cudaStreamSynchronize(st), "msbfs");
+		s->d2h_bytes += sizeof(h);
+		uint64_t qlen = h[0];
+		uint64_t mf = h[1];        // out-degree sum of the frontier, for the direction choice
+		uint64_t mu = sn->out.n_edges > mf ? sn->out.n_edges - mf : 0;
+		int32_t depth = 0;
+		int td = 0, bu = 0;
+		std::vector<int32_t> maxlev(n, 0);
+		bool top_down = true;
+		while (qlen > 0) {
+			if (top_down && has_in && (double)mf > (double)mu / alpha) top_down = false;
+			else if (!top_down && (double)qlen < (double)V / beta) top_down = true;
+			LG_CUDA(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned long long), st), "memset");
+			if (top_down) {
+				list_slots<<<grid_for(qlen, B), B, 0, st>>>(out, q, (uint32_t)qlen, qcnt);
+				LG_TRY(exclusive_scan_u32(qcnt, qpos, qlen, sc[8], st, nullptr));
+				ms_top_down<<<td_blocks, kMsThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, cur,
+						seen, nxt, cand, ctr + 3);
+				unsigned long long nc = 0;
+				LG_CUDA(cudaMemcpyAsync(&nc, ctr + 3, sizeof(nc), cudaMemcpyDeviceToHost, st), "d2h");
+				LG_CUDA(cudaStreamSynchronize(st), "msbfs step");
+				if (nc > 0)
+					ms_commit<<<grid_for(nc, B), B, 0, st>>>(cand, (uint32_t)nc, depth + 1, V, nxt,
+							seen, cur2, plv, outdeg, q2, ctr);
+				td++;
+				s->launches += 5 + (nc > 0);
+			} else {
+				if (fi)
+					ms_bottom_up_flat<<<grid_for(V, kMsThreads * kMsVerts), kMsThreads, 0, st>>>(
+							fi->off.as<uint32_t>(), fi->ids.as<uint32_t>(), (uint32_t)V, lanes,
+							cur, seen, nxt);
+				else
+					ms_bottom_up<<<grid_for(V, kMsThreads), kMsThreads, 0, st>>>(in, lanes, cur,
+							seen, nxt);
+				ms_commit<<<grid_for(V, B), B, 0, st>>>(nullptr, (uint32_t)V, depth + 1, V, nxt,
+						seen, cur2, plv, outdeg, q2, ctr);
+				bu++;
+				s->launches += 2;
+			}
+			ms_clear<<<grid_for(qlen, B), B, 0, st>>>(q, (uint32_t)qlen, cur);
+			LG_CUDA(cudaGetLastError(), "msbfs step");
+			s->launches++;
+			LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+			s->d2h_bytes += sizeof(h) + sizeof(unsigned long long);
+			LG_CUDA(cudaStreamSynchronize(st), "msbfs step");
+			qlen = h[0];
+			mf = h[1];
+			mu -= std::min(mu, (uint64_t)mf);
+			depth++;
+			for (u64 b = h[2]; b; b &= b - 1) maxlev[__builtin_ctzll(b)] = depth;
+			std::swap(q, q2);
+			std::swap(cur, cur2);
+		}
+		if (results) {
+			ms_reach<<<(unsigned)sms * 4u, B, 0, st>>>(seen, outdeg, V, n, lane_cnt, lane_edges);
+			LG_CUDA(cudaGetLastError(), "ms_reach");
+			s->launches++;
+			std::vector<unsigned long long> hc(2 * kMsMaxRoots);
+			LG_CUDA(cudaMemcpyAsync(hc.data(), lane_cnt, hc.size() * sizeof(unsigned long long),
+					cudaMemcpyDeviceToHost, st), "d2h");
+			LG_CUDA(cudaStreamSynchronize(st), "msbfs");
+			s->d2h_bytes += hc.size() * sizeof(unsigned long long);
+			for (int k = 0; k < n; k++) {
+				lg_bfs_result& r = results[p0 + k];
+				r.reached = hc[k];
+				r.reach_edges = hc[kMsMaxRoots + k];
+				r.max_level = maxlev[k];
+				r.top_down_steps = td;
+				r.bottom_up_steps = bu;
+				r.reserved = 0;
+			}
+		}
+	}
+	if (!dev_out) {
+		LG_TRY(copy_out(s, levels, lv, (uint64_t)n_roots * V * sizeof(int32_t)));
+		LG_CUDA(cudaStreamSynchronize(st), "msbfs");
+	}
+	return LG_OK;
+}

@@ -367,6 +367,14 @@ class Snapshot:
         check(lib.lg_bfs(self._h, int(root), ptr(res), C.byref(r)))
         return res, r
 
+    def bfs_multi(self, roots, out=None):
+        """BFS levels from every root in one call: (levels[n][V], results)."""
+        r = np.ascontiguousarray(roots, dtype=np.int64)
+        res = np.empty((len(r), self.max_nodes), np.int32) if out is None else out
+        rs = (_lib.lg_bfs_result * len(r))()
+        check(lib.lg_bfs_multi(self._h, ptr(r), len(r), ptr(res), rs))
+        return res, list(rs)
+
     def scc(self, out=None):
         """Strongly connected components, labelled by their smallest vertex;
         returns (labels, lg_scc_result)."""
