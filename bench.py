@@ -651,12 +651,15 @@ def barrier(ws):
 
 
 def reduce_max_sum(ws, ms, edges):
+    """(max over ranks of ms, sum over ranks of edges): the job's time is its
+    slowest rank's, its work all ranks' work."""
     if ws == 1:
         return ms, edges
     import torch
     import torch.distributed as dist
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    e = torch.tensor([float(edges)], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    e = torch.tensor([float(edges)], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     dist.all_reduce(e, op=dist.ReduceOp.SUM)
     return float(t.item()), float(e.item())
