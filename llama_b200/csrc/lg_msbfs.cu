@@ -166,8 +166,11 @@ ms_bottom_up(SnapCsr in, u64 lanes, const u64* cur, const u64* seen, u64* nxt) {
 // bits become the next frontier (cur2, zero before), are added to seen and
 // get level depth + 1; the vertex joins the next queue.  ctr[0] next queue
 // length, ctr[1] its out-degree sum, ctr[2] OR of the new bits.
+//
+// The level rows are written root by root for all threads of a warp alike,
+// so the lanes holding bit k write row k at consecutive vertices together.
 __global__ void ms_commit(const uint32_t* list, uint32_t n, uint32_t depth1, uint64_t V,
-		u64* nxt, u64* seen, u64* cur2, int32_t* levels, const uint32_t* outdeg,
+		int nroots, u64* nxt, u64* seen, u64* cur2, int32_t* levels, const uint32_t* outdeg,
 		uint32_t* queue, unsigned long long* ctr) {
 	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	uint32_t w = 0;
@@ -181,10 +184,12 @@ __global__ void ms_commit(const uint32_t* list, uint32_t n, uint32_t depth1, uin
 			if (bits) {
 				seen[w] |= bits;
 				cur2[w] = bits;
-				for (u64 b = bits; b; b &= b - 1)
-					levels[(uint64_t)(__ffsll((long long)b) - 1) * V + w] = (int32_t)depth1;
 			}
 		}
+	}
+	if (__any_sync(0xffffffffu, bits != 0)) {
+		for (int k = 0; k < nroots; k++)
+			if ((bits >> k) & 1ull) levels[(uint64_t)k * V + w] = (int32_t)depth1;
 	}
 	ms_push(bits != 0, w, queue, ctr);
 	unsigned long long e = bits ? __ldg(outdeg + w) : 0ull;
@@ -205,27 +210,41 @@ __global__ void ms_clear(const uint32_t* queue, uint32_t n, u64* cur) {
 	if (i < n) cur[__ldg(queue + i)] = 0;
 }
 
-// Per-root reached vertices and the out-degree sum over them.
+// Per-root reached vertices and the out-degree sum over them.  A warp takes
+// 32 vertices at a time and, for every root k, counts the lanes holding bit
+// k (ballot) and adds their out-degrees (warp reductions of the two 16-bit
+// halves, so no sum can overflow); lane k keeps root k's running totals
+// (lane k - 32 for roots 32..63) and adds them to the global counters once.
 __global__ void ms_reach(const u64* seen, const uint32_t* outdeg, uint64_t V, int n,
 		unsigned long long* cnt, unsigned long long* edges) {
-	__shared__ unsigned long long sc[kMsMaxRoots], se[kMsMaxRoots];
-	for (int k = threadIdx.x; k < kMsMaxRoots; k += blockDim.x) { sc[k] = 0; se[k] = 0; }
-	__syncthreads();
-	for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V;
-			v += (uint64_t)gridDim.x * blockDim.x) {
-		u64 b = seen[v];
-		if (!b) continue;
-		const unsigned long long d = __ldg(outdeg + v);
-		for (; b; b &= b - 1) {
-			const int k = __ffsll((long long)b) - 1;
-			atomicAdd(sc + k, 1ull);
-			atomicAdd(se + k, d);
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+	unsigned long long c0 = 0, c1 = 0, e0 = 0, e1 = 0;   // roots lane, lane + 32
+	for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
+		const uint64_t v = base + lane;
+		const u64 b = v < V ? seen[v] : 0ull;
+		if (!__any_sync(0xffffffffu, b != 0)) continue;
+		const uint32_t d = v < V ? __ldg(outdeg + v) : 0u;
+		for (int k = 0; k < n; k++) {
+			const bool has = (b >> k) & 1ull;
+			const uint32_t c = __popc(__ballot_sync(0xffffffffu, has));
+			if (!c) continue;
+			const uint32_t lo = __reduce_add_sync(0xffffffffu, has ? (d & 0xffffu) : 0u);
+			const uint32_t hi = __reduce_add_sync(0xffffffffu, has ? (d >> 16) : 0u);
+			const unsigned long long e = (unsigned long long)lo + ((unsigned long long)hi << 16);
+			if ((uint32_t)(k & 31) == lane) {
+				if (k < 32) { c0 += c; e0 += e; } else { c1 += c; e1 += e; }
+			}
 		}
 	}
-	__syncthreads();
-	for (int k = threadIdx.x; k < n; k += blockDim.x) {
-		if (sc[k]) atomicAdd(cnt + k, sc[k]);
-		if (se[k]) atomicAdd(edges + k, se[k]);
+	if ((int)lane < n) {
+		if (c0) atomicAdd(cnt + lane, c0);
+		if (e0) atomicAdd(edges + lane, e0);
+	}
+	if ((int)lane + 32 < n) {
+		if (c1) atomicAdd(cnt + lane + 32, c1);
+		if (e1) atomicAdd(edges + lane + 32, e1);
 	}
 }
 
@@ -331,7 +350,7 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 				LG_CUDA(cudaMemcpyAsync(&nc, ctr + 3, sizeof(nc), cudaMemcpyDeviceToHost, st), "d2h");
 				LG_CUDA(cudaStreamSynchronize(st), "msbfs step");
 				if (nc > 0)
-					ms_commit<<<grid_for(nc, B), B, 0, st>>>(cand, (uint32_t)nc, depth + 1, V, nxt,
+					ms_commit<<<grid_for(nc, B), B, 0, st>>>(cand, (uint32_t)nc, depth + 1, V, n, nxt,
 							seen, cur2, plv, outdeg, q2, ctr);
 				td++;
 				s->launches += 5 + (nc > 0);
@@ -343,7 +362,7 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 				else
 					ms_bottom_up<<<grid_for(V, kMsThreads), kMsThreads, 0, st>>>(in, lanes, cur,
 							seen, nxt);
-				ms_commit<<<grid_for(V, B), B, 0, st>>>(nullptr, (uint32_t)V, depth + 1, V, nxt,
+				ms_commit<<<grid_for(V, B), B, 0, st>>>(nullptr, (uint32_t)V, depth + 1, V, n, nxt,
 						seen, cur2, plv, outdeg, q2, ctr);
 				bu++;
 				s->launches += 2;
