@@ -14,7 +14,7 @@
 //   3. every oriented edge (a, b) counts |N+(a) & N+(b)|: each triangle is
 //      seen exactly once, at the edge between its two lowest-ranked vertices.
 // The count is an exact integer sum (atomicAdd of per-warp partials).
-#include "lg_device.cuh"
+#include "lg_expand.cuh"
 #include "lg_sort.cuh"
 
 namespace lg {
@@ -32,17 +32,19 @@ __global__ void tc_rank(const uint32_t* out_deg, const uint32_t* in_deg, uint64_
 	if (v < V) rk[v] = out_deg[v] + (in_deg ? in_deg[v] : 0u);
 }
 
+// Every live arc of the out-CSR, over balanced 1024-slot ranges of all
+// vertices' slots (pos = the snapshot's slot prefix), becomes an oriented key.
+constexpr uint32_t kTcRange = 1024;
 __global__ void __launch_bounds__(kTcThreads)
-tc_emit(SnapCsr out, const uint32_t* rk, unsigned long long* keys,
-		unsigned long long* n_keys) {
+tc_emit(SnapCsr out, const uint32_t* pos, uint32_t total, const uint32_t* rk,
+		unsigned long long* keys, unsigned long long* n_keys) {
 	const uint32_t lane = threadIdx.x & 31u;
-	const uint64_t v64 = ((uint64_t)blockIdx.x * (kTcThreads / 32) + (threadIdx.x >> 5)) * 32 + lane;
-	const uint32_t u = (uint32_t)v64;
-	uint32_t cnt = 0, f0 = 0;
-	if (v64 < out.V) cnt = vertex_slots(out, u, &f0);
-	warp_expand(out, cnt, f0,
-		[&](bool act, uint32_t o, uint32_t nbr, uint32_t, uint32_t) {
-			const uint32_t src = __shfl_sync(0xffffffffu, u, o);
+	const uint32_t nranges = (total + kTcRange - 1) / kTcRange;
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (uint32_t r = warp; r < nranges; r += nwarps)
+	range_for_each(out, nullptr, pos, (uint32_t)out.V, total, nranges, kTcRange, r,
+		[&](bool act, uint32_t, uint32_t src, uint32_t nbr, uint32_t, uint32_t) {
 			const bool take = act && nbr != src;
 			unsigned long long key = 0;
 			if (take) {
@@ -71,21 +73,28 @@ __global__ void tc_offsets(const unsigned long long* keys, uint64_t m, uint64_t 
 	for (int64_t v = p + 1; v <= (int64_t)a && v <= (int64_t)V; v++) off[v] = (uint32_t)i;
 }
 
-__device__ __forceinline__ bool bsearch_u32(const unsigned long long* base, uint32_t n,
-		uint32_t x) {
+// adj[i] = target of oriented edge i (the low half of its key): the
+// forward lists as 4-byte ids, half the bytes of the keys.
+__global__ void tc_targets(const unsigned long long* keys, uint64_t m, uint32_t* adj) {
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+			i += (uint64_t)gridDim.x * blockDim.x)
+		adj[i] = (uint32_t)keys[i];
+}
+
+__device__ __forceinline__ bool bsearch_u32(const uint32_t* base, uint32_t n, uint32_t x) {
 	uint32_t lo = 0, hi = n;
 	while (lo < hi) {
 		uint32_t mid = (lo + hi) >> 1;
-		uint32_t y = (uint32_t)__ldg(base + mid);
+		uint32_t y = __ldg(base + mid);
 		if (y < x) lo = mid + 1; else hi = mid;
 	}
-	return lo < n && (uint32_t)__ldg(base + lo) == x;
+	return lo < n && __ldg(base + lo) == x;
 }
 
 constexpr uint32_t kTcSmall = 16;   // lists this short are intersected by one lane
 
 __global__ void __launch_bounds__(kTcThreads)
-tc_count(const unsigned long long* keys, uint64_t m, const uint32_t* off,
+tc_count(const unsigned long long* keys, const uint32_t* adj, uint64_t m, const uint32_t* off,
 		unsigned long long* total) {
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint64_t warp = (uint64_t)blockIdx.x * (kTcThreads / 32) + (threadIdx.x >> 5);
@@ -105,7 +114,7 @@ tc_count(const unsigned long long* keys, uint64_t m, const uint32_t* off,
 		const bool small = la <= kTcSmall;
 		if (e < m && small)
 			for (uint32_t j = 0; j < la; j++)
-				c += bsearch_u32(keys + sb, lb, (uint32_t)__ldg(keys + sa + j));
+				c += bsearch_u32(adj + sb, lb, __ldg(adj + sa + j));
 		unsigned big = __ballot_sync(0xffffffffu, e < m && !small);
 		while (big) {
 			const int src = __ffs(big) - 1;
@@ -115,7 +124,7 @@ tc_count(const unsigned long long* keys, uint64_t m, const uint32_t* off,
 			const uint32_t s1 = __shfl_sync(0xffffffffu, sb, src);
 			const uint32_t n1 = __shfl_sync(0xffffffffu, lb, src);
 			for (uint32_t j = lane; j < n0; j += 32)
-				c += bsearch_u32(keys + s1, n1, (uint32_t)__ldg(keys + s0 + j));
+				c += bsearch_u32(adj + s1, n1, __ldg(adj + s0 + j));
 		}
 	}
 	for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
@@ -135,7 +144,7 @@ extern "C" lg_status lg_triangle_count(lg_snapshot* sn, lg_tc_result* result) {
 	const uint64_t V = sn->V;
 	const uint64_t E = sn->out.n_edges;
 	if (E >= 0xffffffffull) return set_error(LG_ENOTSUP, "more than 2^32-1 live edges");
-	DevBuf rank, keys, tmpk, tmpp, counts, scan_tmp, uniq, flags, off, ctr;
+	DevBuf rank, keys, tmpk, tmpp, counts, scan_tmp, uniq, flags, off, ctr, adj;
 	LG_TRY(rank.reserve(V * 4));
 	LG_TRY(keys.reserve(std::max<uint64_t>(E, 1) * 8));
 	LG_TRY(ctr.reserve(2 * sizeof(unsigned long long)));
@@ -143,8 +152,10 @@ extern "C" lg_status lg_triangle_count(lg_snapshot* sn, lg_tc_result* result) {
 	tc_rank<<<grid_for(V, 256), 256, 0, st>>>(sn->out.deg.as<uint32_t>(),
 			sn->in.present ? sn->in.deg.as<uint32_t>() : nullptr, V, rank.as<uint32_t>());
 	const SnapCsr out = sn->view(0);
-	tc_emit<<<grid_for((V + 31) / 32, kTcThreads / 32), kTcThreads, 0, st>>>(
-			out, rank.as<uint32_t>(), keys.as<unsigned long long>(),
+	int sms = 148;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+	tc_emit<<<(unsigned)sms * 8u, kTcThreads, 0, st>>>(out, sn->out.slot_off.as<uint32_t>(),
+			(uint32_t)sn->out.n_frag_slots, rank.as<uint32_t>(), keys.as<unsigned long long>(),
 			ctr.as<unsigned long long>());
 	LG_CUDA(cudaGetLastError(), "tc_emit");
 	s->launches += 2;
@@ -161,10 +172,13 @@ extern "C" lg_status lg_triangle_count(lg_snapshot* sn, lg_tc_result* result) {
 	LG_TRY(off.reserve((V + 1) * 4));
 	tc_offsets<<<grid_for(m + 1, 256), 256, 0, st>>>(uniq.as<unsigned long long>(), m, V,
 			off.as<uint32_t>());
-	tc_count<<<148 * 16, kTcThreads, 0, st>>>(uniq.as<unsigned long long>(), m,
-			off.as<uint32_t>(), ctr.as<unsigned long long>() + 1);
+	LG_TRY(adj.reserve(std::max<uint64_t>(m, 1) * 4));
+	tc_targets<<<(unsigned)sms * 8u, 256, 0, st>>>(uniq.as<unsigned long long>(), m,
+			adj.as<uint32_t>());
+	tc_count<<<(unsigned)sms * 16u, kTcThreads, 0, st>>>(uniq.as<unsigned long long>(),
+			adj.as<uint32_t>(), m, off.as<uint32_t>(), ctr.as<unsigned long long>() + 1);
 	LG_CUDA(cudaGetLastError(), "tc_count");
-	s->launches += 2;
+	s->launches += 3;
 	unsigned long long t = 0;
 	LG_CUDA(cudaMemcpyAsync(&t, ctr.as<unsigned long long>() + 1, 8, cudaMemcpyDeviceToHost, st), "d2h");
 	LG_CUDA(cudaStreamSynchronize(st), "tc");
