@@ -14,12 +14,7 @@
 // over balanced frontier ranges that also adds sigma[v] into sigma[w] for
 // every down edge; the backward sweep walks each level's out-edges.
 //
-// lg_bc_batched: 64 sources per pass.  Per vertex the pass keeps a 64-byte
-// row of depths, a 512-byte row of sigma and one of delta.  Edges are spread
-// over balanced ranges as in the plain kernels, but each edge of a chunk is
-// then handled by the whole warp with lane j serving sources j and j + 32, so
-// the edge's id is loaded once for 64 traversals and the per-source state is
-// read as coalesced rows.
+// lg_bc_batched (lg_msbfs.cu) runs 64 sources per pass on bit masks.
 #include "lg_device.cuh"
 #include "lg_expand.cuh"
 
@@ -28,8 +23,6 @@ namespace lg {
 constexpr int32_t kBcUnreached = LG_UNREACHED;
 constexpr uint32_t kBcRange = 1024;
 constexpr int kBcThreads = 256;
-constexpr int kLanes = 64;                 // sources per batch
-constexpr uint8_t kNoDepth = 0xff;
 
 __device__ __forceinline__ void bc_push(bool take, uint32_t item, uint32_t* list,
 		unsigned long long* len) {
@@ -101,136 +94,6 @@ __global__ void bc_accumulate(const uint32_t* lvl, uint32_t n, const double* del
 		double* bc) {
 	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	if (i < n) { const uint32_t v = lvl[i]; bc[v] += delta[v]; }
-}
-
-// ---------------------------------------------------------------------------
-// Batched: 64 sources
-// ---------------------------------------------------------------------------
-
-// depth rows: kLanes bytes per vertex; sigma / delta rows: kLanes doubles.
-__global__ void bc64_init(uint8_t* depth, uint64_t V) {
-	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < V * (kLanes / 16)) ((uint4*)depth)[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
-}
-
-__global__ void bc64_sources(const uint32_t* src, int nb, uint8_t* depth, double* sigma,
-		uint32_t* stamp, uint32_t* list, unsigned long long* ctr) {
-	// one thread: sources may repeat, each keeps its own lane
-	if (blockIdx.x != 0 || threadIdx.x != 0) return;
-	unsigned long long n = 0;
-	for (int j = 0; j < nb; j++) {
-		const uint32_t s = src[j];
-		depth[(uint64_t)s * kLanes + j] = 0;
-		sigma[(uint64_t)s * kLanes + j] = 1.0;
-		if (stamp[s] != 1u) { stamp[s] = 1u; list[n++] = s; }
-	}
-	*ctr = n;
-}
-
-__global__ void __launch_bounds__(kBcThreads)
-bc64_forward(SnapCsr out, const uint32_t* fr, const uint32_t* pos, uint32_t n,
-		uint32_t total, uint32_t nranges, uint8_t* depth, double* sigma, uint32_t k,
-		uint32_t* stamp, uint32_t* next, unsigned long long* ctr) {
-	const uint32_t lane = threadIdx.x & 31u;
-	const uint64_t r = (uint64_t)blockIdx.x * (kBcThreads / 32) + (threadIdx.x >> 5);
-	if (r >= nranges) return;
-	range_for_each(out, fr, pos, n, total, nranges, kBcRange, (uint32_t)r,
-		[&](bool act, uint32_t own, uint32_t v, uint32_t w, uint32_t, uint32_t) {
-			unsigned todo = __ballot_sync(0xffffffffu, act);
-			while (todo) {
-				const int t = __ffs(todo) - 1;
-				todo &= todo - 1;
-				const uint32_t tv = __shfl_sync(0xffffffffu, v, t);
-				const uint32_t tw = __shfl_sync(0xffffffffu, w, t);
-				const uint8_t* dv = depth + (uint64_t)tv * kLanes;
-				uint8_t* dw = depth + (uint64_t)tw * kLanes;
-				bool fresh = false;
-#pragma unroll
-				for (int h = 0; h < 2; h++) {
-					const uint32_t j = lane + 32 * h;
-					if (__ldcg(dv + j) == (uint8_t)k) {
-						uint8_t d = __ldcg(dw + j);
-						if (d == kNoDepth) { dw[j] = (uint8_t)(k + 1); d = (uint8_t)(k + 1); fresh = true; }
-						if (d == (uint8_t)(k + 1))
-							atomicAdd(sigma + (uint64_t)tw * kLanes + j,
-									__ldcg(sigma + (uint64_t)tv * kLanes + j));
-					}
-				}
-				if (__any_sync(0xffffffffu, fresh) && lane == 0
-						&& atomicExch(stamp + tw, k + 2) != k + 2) {
-					const unsigned long long p = atomicAdd(ctr, 1ull);
-					next[p] = tw;
-				}
-			}
-		});
-}
-
-__global__ void __launch_bounds__(kBcThreads)
-bc64_backward(SnapCsr out, const uint32_t* fr, const uint32_t* pos, uint32_t n,
-		uint32_t total, uint32_t nranges, const uint8_t* depth, const double* sigma,
-		double* delta, uint32_t k) {
-	const uint32_t lane = threadIdx.x & 31u;
-	const uint64_t r = (uint64_t)blockIdx.x * (kBcThreads / 32) + (threadIdx.x >> 5);
-	if (r >= nranges) return;
-	uint32_t cur = 0xffffffffu;
-	double acc0 = 0.0, acc1 = 0.0;
-	range_for_each(out, fr, pos, n, total, nranges, kBcRange, (uint32_t)r,
-		[&](bool act, uint32_t own, uint32_t v, uint32_t w, uint32_t, uint32_t) {
-			unsigned todo = __ballot_sync(0xffffffffu, act);
-			while (todo) {
-				const int t = __ffs(todo) - 1;
-				todo &= todo - 1;
-				const uint32_t tv = __shfl_sync(0xffffffffu, v, t);
-				const uint32_t tw = __shfl_sync(0xffffffffu, w, t);
-				if (tv != cur) {
-					if (cur != 0xffffffffu) {
-						if (acc0 != 0.0) atomicAdd(delta + (uint64_t)cur * kLanes + lane, acc0);
-						if (acc1 != 0.0) atomicAdd(delta + (uint64_t)cur * kLanes + lane + 32, acc1);
-					}
-					cur = tv;
-					acc0 = acc1 = 0.0;
-				}
-				const uint8_t* dv = depth + (uint64_t)tv * kLanes;
-				const uint8_t* dw = depth + (uint64_t)tw * kLanes;
-#pragma unroll
-				for (int h = 0; h < 2; h++) {
-					const uint32_t j = lane + 32 * h;
-					if (__ldg(dv + j) == (uint8_t)k && __ldg(dw + j) == (uint8_t)(k + 1)) {
-						const double c = __ldg(sigma + (uint64_t)tv * kLanes + j)
-							/ __ldg(sigma + (uint64_t)tw * kLanes + j)
-							* (1.0 + __ldcg(delta + (uint64_t)tw * kLanes + j));
-						if (h == 0) acc0 += c; else acc1 += c;
-					}
-				}
-			}
-		});
-	if (cur != 0xffffffffu) {
-		if (acc0 != 0.0) atomicAdd(delta + (uint64_t)cur * kLanes + lane, acc0);
-		if (acc1 != 0.0) atomicAdd(delta + (uint64_t)cur * kLanes + lane + 32, acc1);
-	}
-}
-
-// bc[v] += sum of delta[v][j] over the sources j that have v at depth k
-// (v != source j); one warp per vertex of the level.
-__global__ void bc64_accumulate(const uint32_t* lvl, uint32_t n, const uint8_t* depth,
-		const double* delta, const uint32_t* src, int nb, uint32_t k, double* bc) {
-	const uint32_t lane = threadIdx.x & 31u;
-	const uint64_t i = (uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-	if (i >= n) return;
-	const uint32_t v = lvl[i];
-	double s = 0.0;
-	for (int h = 0; h < 2; h++) {
-		const uint32_t j = lane + 32 * h;
-		if ((int)j < nb && depth[(uint64_t)v * kLanes + j] == (uint8_t)k && src[j] != v)
-			s += delta[(uint64_t)v * kLanes + j];
-	}
-	for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-	if (lane == 0) bc[v] += s;
-}
-
-__global__ void clear_stamps(uint32_t* stamp, const uint32_t* list, uint64_t n) {
-	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	if (i < n) stamp[list[i]] = 0;
 }
 
 } // namespace lg
@@ -338,100 +201,5 @@ extern "C" lg_status lg_bc(lg_snapshot* sn, const int64_t* sources, int n_source
 	}
 	if (!dev_out) LG_TRY(copy_out(s, bc, acc, V * 8));
 	LG_CUDA(cudaStreamSynchronize(st), "bc");
-	return LG_OK;
-}
-
-extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources,
-		int n_sources, double* bc) {
-	clear_error();
-	if (!bc) return set_error(LG_EINVAL, "null output");
-	LG_TRY(check_sources(sn, sources, n_sources));
-	lg_store* s = sn->store;
-	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
-	cudaStream_t st = s->stream;
-	const uint64_t V = sn->V;
-	DevBuf depth, sigma, delta, stamp, order, cnt, pos, scan_tmp, ctrb, srcb, bcb;
-	LG_TRY(depth.reserve(V * kLanes));
-	LG_TRY(sigma.reserve(V * kLanes * 8));
-	LG_TRY(delta.reserve(V * kLanes * 8));
-	LG_TRY(stamp.reserve(V * 4));
-	LG_TRY(order.reserve(V * 4 * 8 + 64));   // concatenated level lists
-	LG_TRY(cnt.reserve(V * 4));
-	LG_TRY(pos.reserve((V + 1) * 4));
-	LG_TRY(ctrb.reserve(8));
-	LG_TRY(srcb.reserve(kLanes * 4));
-	const bool dev_out = is_device_pointer(bc);
-	double* acc = bc;
-	if (!dev_out) { LG_TRY(bcb.reserve(V * 8)); acc = bcb.as<double>(); }
-	LG_CUDA(cudaMemsetAsync(acc, 0, V * 8, st), "memset");
-	LG_CUDA(cudaMemsetAsync(stamp.p, 0, V * 4, st), "memset");
-	const SnapCsr out = sn->view(0);
-	uint8_t* dp = depth.as<uint8_t>();
-	double* sg = sigma.as<double>();
-	double* dl = delta.as<double>();
-	uint32_t* st_ = stamp.as<uint32_t>();
-	uint32_t* ord = order.as<uint32_t>();
-	const uint64_t ord_cap = V * 8 + 16;
-	unsigned long long* ctr = ctrb.as<unsigned long long>();
-	uint32_t* srcd = srcb.as<uint32_t>();
-	std::vector<uint64_t> off;
-	for (int b0 = 0; b0 < n_sources; b0 += kLanes) {
-		const int nb = std::min(kLanes, n_sources - b0);
-		uint32_t hs[kLanes];
-		for (int j = 0; j < kLanes; j++) hs[j] = j < nb ? (uint32_t)sources[b0 + j] : 0xffffffffu;
-		LG_CUDA(cudaMemcpyAsync(srcd, hs, sizeof(hs), cudaMemcpyHostToDevice, st), "h2d");
-		s->h2d_bytes += sizeof(hs);
-		bc64_init<<<grid_for(V * (kLanes / 16), 256), 256, 0, st>>>(dp, V);
-		LG_CUDA(cudaMemsetAsync(sg, 0, V * kLanes * 8, st), "memset");
-		LG_CUDA(cudaMemsetAsync(dl, 0, V * kLanes * 8, st), "memset");
-		bc64_sources<<<1, 32, 0, st>>>(srcd, nb, dp, sg, st_, ord, ctr);
-		s->launches += 2;
-		uint64_t n0 = 0;
-		LG_TRY(read_u64(s, ctr, &n0));
-		off.assign({0, n0});
-		for (uint32_t k = 0;; k++) {
-			const uint64_t b = off[k], n = off[k + 1] - off[k];
-			if (n == 0) break;
-			if (k + 2 >= 0xff) return set_error(LG_ENOTSUP, "BFS deeper than 253 levels");
-			if (off[k + 1] + V > ord_cap)
-				return set_error(LG_ENOTSUP, "level lists exceed their buffer");
-			uint64_t total = 0;
-			LG_TRY(list_offsets(s, out, ord + b, (uint32_t)n, cnt, pos, scan_tmp, &total));
-			LG_CUDA(cudaMemsetAsync(ctr, 0, 8, st), "memset");
-			const uint32_t nr = (uint32_t)((total + kBcRange - 1) / kBcRange);
-			if (nr) {
-				bc64_forward<<<grid_for(nr, kBcThreads / 32), kBcThreads, 0, st>>>(out, ord + b,
-						pos.as<uint32_t>(), (uint32_t)n, (uint32_t)total, nr, dp, sg, k, st_,
-						ord + off[k + 1], ctr);
-				s->launches++;
-			}
-			LG_CUDA(cudaGetLastError(), "bc64_forward");
-			uint64_t produced = 0;
-			LG_TRY(read_u64(s, ctr, &produced));
-			off.push_back(off[k + 1] + produced);
-		}
-		// levels D-1 .. 1; level 0 holds only the sources, which BC excludes
-		const int D = (int)off.size() - 2;
-		for (int k = D - 1; k >= 1; k--) {
-			const uint64_t b = off[k], n = off[k + 1] - off[k];
-			uint64_t total = 0;
-			LG_TRY(list_offsets(s, out, ord + b, (uint32_t)n, cnt, pos, scan_tmp, &total));
-			const uint32_t nr = (uint32_t)((total + kBcRange - 1) / kBcRange);
-			if (nr && k < D - 1) {
-				bc64_backward<<<grid_for(nr, kBcThreads / 32), kBcThreads, 0, st>>>(out, ord + b,
-						pos.as<uint32_t>(), (uint32_t)n, (uint32_t)total, nr, dp, sg, dl, k);
-				s->launches++;
-			}
-			bc64_accumulate<<<grid_for(n, 8), 256, 0, st>>>(ord + b, (uint32_t)n, dp, dl,
-					srcd, nb, k, acc);
-			s->launches++;
-			LG_CUDA(cudaGetLastError(), "bc64_backward");
-		}
-		// reset the stamps of every listed vertex for the next batch
-		clear_stamps<<<grid_for(off.back(), 256), 256, 0, st>>>(st_, ord, off.back());
-		s->launches++;
-	}
-	if (!dev_out) LG_TRY(copy_out(s, bc, acc, V * 8));
-	LG_CUDA(cudaStreamSynchronize(st), "bc batched");
 	return LG_OK;
 }

@@ -18,6 +18,9 @@
 // missing root is found; flat in-CSR when the snapshot has one).  A commit
 // pass turns nxt into the new frontier, sets seen, and writes depth + 1 into
 // the level arrays of the new roots' bits.
+//
+// lg_bc_batched runs Brandes' betweenness centrality on the same machinery,
+// 64 sources per pass (see the section below).
 #include "lg_expand.cuh"
 #include "lg_flat.cuh"
 
@@ -187,7 +190,7 @@ __global__ void ms_commit(const uint32_t* list, uint32_t n, uint32_t depth1, uin
 			}
 		}
 	}
-	if (__any_sync(0xffffffffu, bits != 0)) {
+	if (levels && __any_sync(0xffffffffu, bits != 0)) {
 		for (int k = 0; k < nroots; k++)
 			if ((bits >> k) & 1ull) levels[(uint64_t)k * V + w] = (int32_t)depth1;
 	}
@@ -248,9 +251,327 @@ __global__ void ms_reach(const u64* seen, const uint32_t* outdeg, uint64_t V, in
 	}
 }
 
+// ---------------------------------------------------------------------------
+// Batched Brandes betweenness centrality
+//
+// Reference: ll_b_bc_random (benchmark/benchmarks/bc_random.h:55-193): per
+// source s, sigma is pushed along down edges (depth[w] == depth[v] + 1,
+// ll_bfs_template.h:337-351) and the reverse sweep, deepest level first, sets
+//   delta[v] = sum over down edges v->w of sigma[v] / sigma[w] * (1 + delta[w])
+// and BC[v] += delta[v] for v != s (bc_random.h:73-111), in FP32 there and
+// FP64 here.  A pass serves 64 sources: the BFS levels are the multi-source
+// BFS above (lk[v] = the sources that have v at depth k, kept for every
+// depth), and sigma / delta are 64 doubles per vertex.  An edge v->w is a
+// down edge for exactly the sources in lk[v] & lk+1[w], so a sweep over the
+// out-edges of a level reads one 8-byte mask per edge and touches sigma and
+// delta only for those sources: the work follows the (source, down edge)
+// pairs, not 64 x every edge.  Sums use FP64 atomics, so results agree with
+// an exact evaluation to ~1e-15 relative, not bit for bit.
+// ---------------------------------------------------------------------------
+
+// Sources of a pass: level-0 masks, sigma = 1, the sources' own-lane mask.
+__global__ void bcm_roots(const int64_t* src, int n, u64* seen, u64* l0, u64* own,
+		double* sigma, uint32_t* queue, unsigned long long* ctr, const uint32_t* outdeg) {
+	const int k = threadIdx.x;
+	if (k >= n) return;
+	const uint32_t v = (uint32_t)src[k];
+	atomicOr(seen + v, 1ull << k);
+	atomicOr(own + v, 1ull << k);
+	sigma[(uint64_t)v * kMsMaxRoots + k] = 1.0;
+	const u64 old = atomicOr(l0 + v, 1ull << k);
+	if (old == 0) {
+		queue[atomicAdd(ctr, 1ull)] = v;
+		atomicAdd(ctr + 1, (unsigned long long)__ldg(outdeg + v));
+	}
+}
+
+// sigma[w][j] += sigma[v][j] over the out-edges v->w of level k's vertices
+// for the sources j in lk[v] & lk1[w]; the warp takes such edges one at a
+// time, lane j serving sources j and j + 32.
+__global__ void __launch_bounds__(kMsThreads)
+bcm_sigma(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
+		const u64* lk, const u64* lk1, double* sigma) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t total = __ldg(pos + qlen);
+	const uint32_t nranges = (total + kMsRange - 1) / kMsRange;
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (uint32_t r = warp; r < nranges; r += nwarps) {
+		range_for_each(out, queue, pos, qlen, total, nranges, kMsRange, r,
+			[&](bool act, uint32_t, uint32_t v, uint32_t w, uint32_t, uint32_t) {
+				const u64 m = act ? (__ldg(lk + v) & __ldg(lk1 + w)) : 0ull;
+				unsigned todo = __ballot_sync(0xffffffffu, m != 0);
+				while (todo) {
+					const int t = __ffs(todo) - 1;
+					todo &= todo - 1;
+					const uint32_t tv = __shfl_sync(0xffffffffu, v, t);
+					const uint32_t tw = __shfl_sync(0xffffffffu, w, t);
+					const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)m, t);
+					const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(m >> 32), t);
+					const double* sv = sigma + (uint64_t)tv * kMsMaxRoots;
+					double* sw = sigma + (uint64_t)tw * kMsMaxRoots;
+					if ((lo >> lane) & 1u) atomicAdd(sw + lane, __ldcg(sv + lane));
+					if ((hi >> lane) & 1u) atomicAdd(sw + 32 + lane, __ldcg(sv + 32 + lane));
+				}
+			});
+	}
+}
+
+// delta[v][j] = sum over down edges v->w (j in lk[v] & lk1[w]) of
+// sigma[v][j] * q[w][j], for level k's vertices, where q[w][j] =
+// (1 + delta[w][j]) / sigma[w][j] has already replaced sigma[w][j] for the
+// sources that have w at depth k + 1 (bcm_quot), so an edge costs a multiply,
+// not a division; edges come grouped by v, so each lane keeps v's two partial
+// sums and adds them to delta once per run of v.
+__global__ void __launch_bounds__(kMsThreads)
+bcm_delta(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
+		const u64* lk, const u64* lk1, const double* sigma, double* delta) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t total = __ldg(pos + qlen);
+	const uint32_t nranges = (total + kMsRange - 1) / kMsRange;
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (uint32_t r = warp; r < nranges; r += nwarps) {
+		uint32_t cur = 0xffffffffu;
+		double a0 = 0.0, a1 = 0.0;
+		range_for_each(out, queue, pos, qlen, total, nranges, kMsRange, r,
+			[&](bool act, uint32_t, uint32_t v, uint32_t w, uint32_t, uint32_t) {
+				const u64 m = act ? (__ldg(lk + v) & __ldg(lk1 + w)) : 0ull;
+				unsigned todo = __ballot_sync(0xffffffffu, m != 0);
+				while (todo) {
+					const int t = __ffs(todo) - 1;
+					todo &= todo - 1;
+					const uint32_t tv = __shfl_sync(0xffffffffu, v, t);
+					const uint32_t tw = __shfl_sync(0xffffffffu, w, t);
+					const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)m, t);
+					const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(m >> 32), t);
+					if (tv != cur) {
+						if (cur != 0xffffffffu) {
+							double* dv = delta + (uint64_t)cur * kMsMaxRoots;
+							if (a0 != 0.0) atomicAdd(dv + lane, a0);
+							if (a1 != 0.0) atomicAdd(dv + 32 + lane, a1);
+						}
+						cur = tv;
+						a0 = a1 = 0.0;
+					}
+					const double* sv = sigma + (uint64_t)tv * kMsMaxRoots;
+					const double* qw = sigma + (uint64_t)tw * kMsMaxRoots;
+					if ((lo >> lane) & 1u) a0 += __ldg(sv + lane) * __ldg(qw + lane);
+					if ((hi >> lane) & 1u) a1 += __ldg(sv + 32 + lane) * __ldg(qw + 32 + lane);
+				}
+			});
+		if (cur != 0xffffffffu) {
+			double* dv = delta + (uint64_t)cur * kMsMaxRoots;
+			if (a0 != 0.0) atomicAdd(dv + lane, a0);
+			if (a1 != 0.0) atomicAdd(dv + 32 + lane, a1);
+		}
+	}
+}
+
+// For the vertices of a level whose delta is final: sigma[w][j] <-
+// (1 + delta[w][j]) / sigma[w][j] for the sources j in lk[w] (the factor the
+// level above multiplies by).  A warp per vertex, lane j serving j and j + 32.
+__global__ void bcm_quot(const uint32_t* queue, uint32_t n, const u64* lk, double* sigma,
+		const double* delta) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	if (i >= n) return;
+	const uint32_t w = __ldg(queue + i);
+	const u64 m = __ldg(lk + w);
+	double* sw = sigma + (uint64_t)w * kMsMaxRoots;
+	const double* dw = delta + (uint64_t)w * kMsMaxRoots;
+	if ((m >> lane) & 1ull) sw[lane] = (1.0 + dw[lane]) / sw[lane];
+	if ((m >> (lane + 32)) & 1ull) sw[32 + lane] = (1.0 + dw[32 + lane]) / sw[32 + lane];
+}
+
+// bc[v] += delta[v][j] over the sources j that reached v, v not being j's
+// source, in increasing j.
+__global__ void bcm_accum(const u64* seen, const u64* own, const double* delta, uint64_t V,
+		double* bc) {
+	const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (v >= V) return;
+	u64 b = seen[v] & ~own[v];
+	if (!b) return;
+	const double* dv = delta + v * kMsMaxRoots;
+	double sum = 0.0;
+	for (; b; b &= b - 1) sum += dv[__ffsll((long long)b) - 1];
+	bc[v] += sum;
+}
+
 } // namespace lg
 
 using namespace lg;
+
+namespace {
+
+// Grows b to hold `need` bytes keeping its first `keep` bytes.
+lg_status grow_keep(DevBuf& b, size_t need, size_t keep, cudaStream_t st) {
+	if (need <= b.bytes) return LG_OK;
+	DevBuf nb;
+	LG_TRY(nb.reserve(std::max(need, b.bytes * 2)));
+	if (keep) LG_CUDA(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice, st), "grow");
+	LG_CUDA(cudaStreamSynchronize(st), "grow");
+	b.swap(nb);
+	return LG_OK;
+}
+
+} // namespace
+
+extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int n_sources,
+		double* bc) {
+	clear_error();
+	if (!sn || !bc || (!sources && n_sources > 0)) return set_error(LG_EINVAL, "null argument");
+	if (n_sources < 0) return set_error(LG_EINVAL, "negative source count");
+	for (int i = 0; i < n_sources; i++)
+		if (sources[i] < 0 || (uint64_t)sources[i] >= sn->V)
+			return set_error(LG_EINVAL, "source %lld out of range", (long long)sources[i]);
+	lg_store* s = sn->store;
+	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+	cudaStream_t st = s->stream;
+	const uint64_t V = sn->V;
+	const unsigned B = 256;
+	DevBuf* sc = s->scratch;
+	LG_TRY(sc[0].reserve(3 * V * sizeof(u64)));                        // seen, nxt, own
+	LG_TRY(sc[1].reserve(2 * V * kMsMaxRoots * sizeof(double)));       // sigma, delta
+	LG_TRY(sc[3].reserve(V * sizeof(uint32_t)));                       // candidates
+	LG_TRY(sc[5].reserve((2 * V + 1) * sizeof(uint32_t)));             // slot counts, prefix
+	LG_TRY(sc[6].reserve(8 * sizeof(unsigned long long)));
+	LG_TRY(sc[7].reserve(kMsMaxRoots * sizeof(int64_t)));
+	u64* seen = sc[0].as<u64>();
+	u64* nxt = seen + V;
+	u64* own = nxt + V;
+	double* sigma = sc[1].as<double>();
+	double* delta = sigma + V * kMsMaxRoots;
+	uint32_t* cand = sc[3].as<uint32_t>();
+	uint32_t* qcnt = sc[5].as<uint32_t>();
+	uint32_t* qpos = qcnt + V;
+	unsigned long long* ctr = sc[6].as<unsigned long long>();
+	DevBuf& masks = sc[2];          // level masks, V per level
+	DevBuf& queues = sc[4];         // level queues, concatenated
+	LG_TRY(grow_keep(masks, 8 * V * sizeof(u64), 0, st));
+	LG_TRY(grow_keep(queues, 4 * V * sizeof(uint32_t), 0, st));
+	const bool dev_out = is_device_pointer(bc);
+	double* acc = bc;
+	if (!dev_out) { LG_TRY(sc[8].reserve(V * sizeof(double))); acc = sc[8].as<double>(); }
+	LG_CUDA(cudaMemsetAsync(acc, 0, V * sizeof(double), st), "clear bc");
+	const FlatCsr* fi = sn->flat[1];
+	const FlatCsr* fo = sn->flat[0];
+	const SnapCsr out = (fo && fo->has_view) ? fo->view(sn->out.deg.as<uint32_t>()) : sn->view(0);
+	const bool has_in = sn->in.present;
+	const SnapCsr in = has_in ? sn->view(1) : out;
+	if (!fi && has_in && n_sources > 0) {
+		// the bottom-up steps read in-edges many times per pass: flatten them
+		// for the call unless the snapshot already holds a flat in-CSR
+		if (!s->flat_scratch) s->flat_scratch = new FlatCsr;
+		LG_TRY(build_flat(sn, 1, *s->flat_scratch, false));
+		fi = s->flat_scratch;
+	}
+	const uint32_t* outdeg = sn->out.deg.as<uint32_t>();
+	int sms = 148;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+	const unsigned grid = (unsigned)sms * 8u;
+	const double alpha = 14.0, beta = 24.0;
+
+	for (int p0 = 0; p0 < n_sources; p0 += kMsMaxRoots) {
+		const int n = std::min(kMsMaxRoots, n_sources - p0);
+		const u64 lanes = n == 64 ? ~0ull : ((1ull << n) - 1ull);
+		LG_CUDA(cudaMemsetAsync(seen, 0, 3 * V * sizeof(u64), st), "clear masks");
+		LG_CUDA(cudaMemsetAsync(sigma, 0, 2 * V * kMsMaxRoots * sizeof(double), st), "clear");
+		LG_CUDA(cudaMemsetAsync(masks.p, 0, 2 * V * sizeof(u64), st), "clear level masks");
+		LG_CUDA(cudaMemsetAsync(ctr, 0, 8 * sizeof(unsigned long long), st), "clear counters");
+		LG_CUDA(cudaMemcpyAsync(sc[7].p, sources + p0, n * sizeof(int64_t),
+				cudaMemcpyHostToDevice, st), "sources");
+		s->h2d_bytes += n * sizeof(int64_t);
+		bcm_roots<<<1, kMsMaxRoots, 0, st>>>(sc[7].as<int64_t>(), n, seen, masks.as<u64>(), own,
+				sigma, queues.as<uint32_t>(), ctr, outdeg);
+		LG_CUDA(cudaGetLastError(), "bcm_roots");
+		s->launches++;
+		unsigned long long h[3];
+		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+		LG_CUDA(cudaStreamSynchronize(st), "bc batched");
+		s->d2h_bytes += sizeof(h);
+		std::vector<uint64_t> qoff = {0, h[0]};   // level k's queue: [qoff[k], qoff[k+1])
+		uint64_t mf = h[1];
+		uint64_t mu = sn->out.n_edges > mf ? sn->out.n_edges - mf : 0;
+		bool top_down = true;
+		// forward: depths, then sigma, level by level
+		for (uint32_t k = 0;; k++) {
+			const uint64_t qb = qoff[k], qlen = qoff[k + 1] - qoff[k];
+			if (qlen == 0) break;
+			LG_TRY(grow_keep(masks, (uint64_t)(k + 3) * V * sizeof(u64),
+					(uint64_t)(k + 2) * V * sizeof(u64), st));
+			LG_TRY(grow_keep(queues, (qoff[k + 1] + V) * sizeof(uint32_t),
+					qoff[k + 1] * sizeof(uint32_t), st));
+			u64* lk = masks.as<u64>() + (uint64_t)k * V;
+			u64* lk1 = lk + V;
+			LG_CUDA(cudaMemsetAsync(lk1 + V, 0, V * sizeof(u64), st), "clear level masks");
+			uint32_t* q = queues.as<uint32_t>() + qb;
+			uint32_t* q2 = queues.as<uint32_t>() + qoff[k + 1];
+			list_slots<<<grid_for(qlen, B), B, 0, st>>>(out, q, (uint32_t)qlen, qcnt);
+			LG_TRY(exclusive_scan_u32(qcnt, qpos, qlen, sc[9], st, nullptr));
+			if (top_down && has_in && (double)mf > (double)mu / alpha) top_down = false;
+			else if (!top_down && (double)qlen < (double)V / beta) top_down = true;
+			LG_CUDA(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned long long), st), "memset");
+			if (top_down) {
+				ms_top_down<<<grid, kMsThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, lk, seen,
+						nxt, cand, ctr + 3);
+				unsigned long long nc = 0;
+				LG_CUDA(cudaMemcpyAsync(&nc, ctr + 3, sizeof(nc), cudaMemcpyDeviceToHost, st), "d2h");
+				LG_CUDA(cudaStreamSynchronize(st), "bc batched");
+				if (nc > 0)
+					ms_commit<<<grid_for(nc, B), B, 0, st>>>(cand, (uint32_t)nc, k + 1, V, n, nxt,
+							seen, lk1, nullptr, outdeg, q2, ctr);
+				s->launches += 5 + (nc > 0);
+			} else {
+				if (fi)
+					ms_bottom_up_flat<<<grid_for(V, kMsThreads * kMsVerts), kMsThreads, 0, st>>>(
+							fi->off.as<uint32_t>(), fi->ids.as<uint32_t>(), (uint32_t)V, lanes,
+							lk, seen, nxt);
+				else
+					ms_bottom_up<<<grid_for(V, kMsThreads), kMsThreads, 0, st>>>(in, lanes, lk,
+							seen, nxt);
+				ms_commit<<<grid_for(V, B), B, 0, st>>>(nullptr, (uint32_t)V, k + 1, V, n, nxt,
+						seen, lk1, nullptr, outdeg, q2, ctr);
+				s->launches += 5;
+			}
+			bcm_sigma<<<grid, kMsThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, lk, lk1, sigma);
+			LG_CUDA(cudaGetLastError(), "bc batched forward");
+			s->launches++;
+			LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+			LG_CUDA(cudaStreamSynchronize(st), "bc batched");
+			s->d2h_bytes += sizeof(h) + sizeof(unsigned long long);
+			qoff.push_back(qoff[k + 1] + h[0]);
+			mf = h[1];
+			mu -= std::min(mu, (uint64_t)mf);
+		}
+		// backward, deepest level with down edges first; level 0 holds only
+		// the sources, whose own delta BC leaves out
+		const int D = (int)qoff.size() - 1;           // levels 0 .. D-1 are non-empty
+		for (int k = D - 1; k >= 1; k--) {
+			const uint64_t qb = qoff[k], qlen = qoff[k + 1] - qoff[k];
+			const u64* lk = masks.as<u64>() + (uint64_t)k * V;
+			const uint32_t* q = queues.as<uint32_t>() + qb;
+			if (k < D - 1) {                          // the deepest level has no down edges
+				list_slots<<<grid_for(qlen, B), B, 0, st>>>(out, q, (uint32_t)qlen, qcnt);
+				LG_TRY(exclusive_scan_u32(qcnt, qpos, qlen, sc[9], st, nullptr));
+				bcm_delta<<<grid, kMsThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, lk, lk + V,
+						sigma, delta);
+				s->launches += 5;
+			}
+			if (k > 1) {                              // level k - 1 multiplies by these
+				bcm_quot<<<grid_for(qlen * 32, B), B, 0, st>>>(q, (uint32_t)qlen, lk, sigma, delta);
+				s->launches++;
+			}
+			LG_CUDA(cudaGetLastError(), "bc batched backward");
+		}
+		bcm_accum<<<grid_for(V, B), B, 0, st>>>(seen, own, delta, V, acc);
+		LG_CUDA(cudaGetLastError(), "bcm_accum");
+		s->launches++;
+	}
+	if (!dev_out) LG_TRY(copy_out(s, bc, acc, V * sizeof(double)));
+	LG_CUDA(cudaStreamSynchronize(st), "bc batched");
+	return LG_OK;
+}
 
 extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_roots,
 		int32_t* levels, lg_bfs_result* results) {
