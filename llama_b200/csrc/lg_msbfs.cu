@@ -94,7 +94,10 @@ ms_top_down(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t ql
 // Bottom-up over a flat in-CSR: a thread takes kBuVerts vertices (blockDim
 // apart) and ORs cur[] over kMsChunk in-neighbours of each per round until
 // every root that has not reached the vertex is found, or the list ends.
+// Vertices with more than kMsHeavy in-edges are left to ms_bottom_up_heavy,
+// so no thread walks a hub's list alone.
 constexpr int kMsVerts = 4;
+constexpr uint32_t kMsHeavy = 512;
 __global__ void __launch_bounds__(kMsThreads)
 ms_bottom_up_flat(const uint32_t* off, const uint32_t* ids, uint32_t V, u64 lanes,
 		const u64* cur, const u64* seen, u64* nxt) {
@@ -107,7 +110,11 @@ ms_bottom_up_flat(const uint32_t* off, const uint32_t* ids, uint32_t V, u64 lane
 		k[j] = 0; end[j] = 0; need[j] = 0; got[j] = 0;
 		if (v < V) {
 			need[j] = lanes & ~seen[v];
-			if (need[j]) { k[j] = __ldg(off + v); end[j] = __ldg(off + v + 1); }
+			if (need[j]) {
+				k[j] = __ldg(off + v);
+				end[j] = __ldg(off + v + 1);
+				if (end[j] - k[j] > kMsHeavy) { end[j] = k[j]; need[j] = 0; }
+			}
 		}
 	}
 	bool more = true;
@@ -139,6 +146,45 @@ ms_bottom_up_flat(const uint32_t* off, const uint32_t* ids, uint32_t V, u64 lane
 		const uint32_t v = base + j * kMsThreads;
 		const u64 b = got[j] & need[j];
 		if (b) nxt[v] = b;
+	}
+}
+
+// Vertices of a flat in-CSR with more than kMsHeavy in-edges.
+__global__ void ms_heavy_list(const uint32_t* off, uint32_t V, uint32_t* list,
+		unsigned long long* n) {
+	const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	const bool h = v < V && __ldg(off + v + 1) - __ldg(off + v) > kMsHeavy;
+	ms_push(h, (uint32_t)v, list, n);
+}
+
+// Bottom-up for the heavy vertices (*nheavy of them in `list`): a warp per
+// vertex ORs the frontier masks of 32 in-neighbours at a time until every
+// root that has not reached the vertex is found, or the list ends.
+__global__ void __launch_bounds__(kMsThreads)
+ms_bottom_up_heavy(const uint32_t* off, const uint32_t* ids, const uint32_t* list,
+		const unsigned long long* nheavy, u64 lanes, const u64* cur, const u64* seen, u64* nxt) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+	const uint64_t n = *nheavy;
+	for (uint64_t i = warp; i < n; i += nwarps) {
+		const uint32_t v = __ldg(list + i);
+		const u64 need = lanes & ~seen[v];
+		if (!need) continue;
+		const uint32_t k1 = __ldg(off + v + 1);
+		u64 got = 0;
+		for (uint32_t b = __ldg(off + v); b < k1; b += 32u * kMsChunk) {
+			u64 f = 0;
+#pragma unroll
+			for (int c = 0; c < kMsChunk; c++) {
+				const uint32_t k = b + c * 32u + lane;
+				if (k < k1) f |= __ldg(cur + __ldg(ids + k));
+			}
+			got |= ((u64)__reduce_or_sync(0xffffffffu, (uint32_t)(f >> 32)) << 32)
+				| __reduce_or_sync(0xffffffffu, (uint32_t)f);
+			if ((got & need) == need) break;
+		}
+		if (lane == 0 && (got & need)) nxt[v] = got & need;
 	}
 }
 
@@ -415,6 +461,21 @@ lg_status grow_keep(DevBuf& b, size_t need, size_t keep, cudaStream_t st) {
 	return LG_OK;
 }
 
+// The vertices of flat in-CSR f with more than kMsHeavy in-edges, listed in
+// buf (a device counter, then the ids) for ms_bottom_up_heavy.
+lg_status heavy_list(lg_store* s, const FlatCsr* f, uint64_t V, DevBuf& buf,
+		uint32_t** list, unsigned long long** count) {
+	LG_TRY(buf.reserve(sizeof(unsigned long long) + std::max<uint64_t>(V, 1) * sizeof(uint32_t)));
+	*count = buf.as<unsigned long long>();
+	*list = reinterpret_cast<uint32_t*>(*count + 1);
+	LG_CUDA(cudaMemsetAsync(*count, 0, sizeof(unsigned long long), s->stream), "clear");
+	ms_heavy_list<<<grid_for(V, 256), 256, 0, s->stream>>>(f->off.as<uint32_t>(), (uint32_t)V,
+			*list, *count);
+	LG_CUDA(cudaGetLastError(), "ms_heavy_list");
+	s->launches++;
+	return LG_OK;
+}
+
 } // namespace
 
 extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int n_sources,
@@ -471,6 +532,9 @@ extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int 
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
 	const unsigned grid = (unsigned)sms * 8u;
 	const double alpha = 14.0, beta = 24.0;
+	uint32_t* hlist = nullptr;
+	unsigned long long* hcount = nullptr;
+	if (fi) LG_TRY(heavy_list(s, fi, V, sc[10], &hlist, &hcount));
 
 	for (int p0 = 0; p0 < n_sources; p0 += kMsMaxRoots) {
 		const int n = std::min(kMsMaxRoots, n_sources - p0);
@@ -523,11 +587,14 @@ extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int 
 							seen, lk1, nullptr, outdeg, q2, ctr);
 				s->launches += 5 + (nc > 0);
 			} else {
-				if (fi)
+				if (fi) {
 					ms_bottom_up_flat<<<grid_for(V, kMsThreads * kMsVerts), kMsThreads, 0, st>>>(
 							fi->off.as<uint32_t>(), fi->ids.as<uint32_t>(), (uint32_t)V, lanes,
 							lk, seen, nxt);
-				else
+					ms_bottom_up_heavy<<<grid, kMsThreads, 0, st>>>(fi->off.as<uint32_t>(),
+							fi->ids.as<uint32_t>(), hlist, hcount, lanes, lk, seen, nxt);
+					s->launches++;
+				} else
 					ms_bottom_up<<<grid_for(V, kMsThreads), kMsThreads, 0, st>>>(in, lanes, lk,
 							seen, nxt);
 				ms_commit<<<grid_for(V, B), B, 0, st>>>(nullptr, (uint32_t)V, k + 1, V, n, nxt,
@@ -622,6 +689,9 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
 	const unsigned td_blocks = (unsigned)sms * 8u;
 	const double alpha = 14.0, beta = 24.0;
+	uint32_t* hlist = nullptr;
+	unsigned long long* hcount = nullptr;
+	if (fi) LG_TRY(heavy_list(s, fi, V, sc[10], &hlist, &hcount));
 
 	ms_fill<<<(unsigned)sms * 16u, B, 0, st>>>(lv, (uint64_t)n_roots * V);
 	LG_CUDA(cudaGetLastError(), "ms_fill");
@@ -676,11 +746,14 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 				td++;
 				s->launches += 5 + (nc > 0);
 			} else {
-				if (fi)
+				if (fi) {
 					ms_bottom_up_flat<<<grid_for(V, kMsThreads * kMsVerts), kMsThreads, 0, st>>>(
 							fi->off.as<uint32_t>(), fi->ids.as<uint32_t>(), (uint32_t)V, lanes,
 							cur, seen, nxt);
-				else
+					ms_bottom_up_heavy<<<td_blocks, kMsThreads, 0, st>>>(fi->off.as<uint32_t>(),
+							fi->ids.as<uint32_t>(), hlist, hcount, lanes, cur, seen, nxt);
+					s->launches++;
+				} else
 					ms_bottom_up<<<grid_for(V, kMsThreads), kMsThreads, 0, st>>>(in, lanes, cur,
 							seen, nxt);
 				ms_commit<<<grid_for(V, B), B, 0, st>>>(nullptr, (uint32_t)V, depth + 1, V, n, nxt,
