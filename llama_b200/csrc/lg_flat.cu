@@ -177,6 +177,7 @@ lg_status build_flat(lg_snapshot* sn, int dir, FlatCsr& f, bool view) {
 
 	f.V = V;
 	f.has_view = false;
+	f.has_nz_outdeg = false;
 	LG_TRY(f.blk.reserve(2ull * (sp.nranges + 1) * sizeof(uint32_t)));
 	uint32_t* blk_live = f.blk.as<uint32_t>();
 	uint32_t* blk_base = blk_live + sp.nranges + 1;

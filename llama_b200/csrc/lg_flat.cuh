@@ -171,6 +171,8 @@ struct FlatCsr {
 	DevBuf rows;               // nz_rows[R] nz_off[R] tile_seg[ntiles] heads[ntiles*8+1]
 	DevBuf blk, flags, scan_tmp, err;   // build scratch
 	DevBuf vfrags, vdel, vlt;  // one-fragment-per-vertex view
+	DevBuf nz_outdeg;          // R u32: out-degree of each row (PageRank, built on use)
+	bool has_nz_outdeg = false;
 	uint64_t rcap() const { return R > 0 ? R : 1; }
 	const uint32_t* nz_rows() const { return rows.as<uint32_t>(); }
 	const uint32_t* nz_off() const { return rows.as<uint32_t>() + rcap(); }

@@ -48,6 +48,7 @@ struct FlatArgs {
 	const uint32_t* ids;       // E
 	const uint32_t* heads;     // ntiles * kFlatTileWords + 1 words
 	const uint32_t* nz_rows;   // R
+	const uint32_t* nz_outdeg; // R: out-degree of nz_rows[k]
 	const uint32_t* nz_off;    // R
 	const uint32_t* tile_seg;  // ntiles
 	uint32_t E, R, ntiles;
@@ -64,7 +65,7 @@ struct FlatArgs {
 __device__ __forceinline__ void flat_finish(const FlatArgs& a, uint32_t k, double s) {
 	const uint32_t v = __ldg(a.nz_rows + k);
 	const double pr = __dadd_rn(a.base, __dmul_rn(a.d, s));
-	const uint32_t dg = __ldg(a.outdeg + v);
+	const uint32_t dg = __ldg(a.nz_outdeg + k);
 	a.contrib_next[v] = dg ? pr / (double)dg : 0.0;
 	if (a.pr_out) a.pr_out[v] = pr;
 }
@@ -210,6 +211,13 @@ __global__ void pr_flat_fixup(FlatArgs a) {
 		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
 		if (lane == 0) flat_finish(a, kk, __ldcg(a.carry_last + tt - 1) + s);
 	}
+}
+
+// nz_outdeg[k] = out-degree of row k's vertex (rows read it in order).
+__global__ void pr_row_degrees(const uint32_t* nz_rows, uint32_t R, const uint32_t* outdeg,
+		uint32_t* nz_outdeg) {
+	const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+	if (k < R) nz_outdeg[k] = __ldg(outdeg + __ldg(nz_rows + k));
 }
 
 // Vertices without in-edges: rank pr, contrib pr / out_degree.
@@ -386,11 +394,21 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 
 	// flat in-adjacency: the snapshot's own (lg_snapshot_flatten) or one
 	// built for this call in store scratch
-	const FlatCsr* f = sn->flat[1];
+	FlatCsr* f = sn->flat[1];
 	if (!f) {
 		if (!s->flat_scratch) s->flat_scratch = new FlatCsr;
 		LG_TRY(build_flat(sn, 1, *s->flat_scratch, false));
 		f = s->flat_scratch;
+	}
+	if (!f->has_nz_outdeg) {
+		LG_TRY(f->nz_outdeg.reserve(f->rcap() * sizeof(uint32_t)));
+		if (f->R > 0) {
+			pr_row_degrees<<<grid_for(f->R, B), B, 0, st>>>(f->nz_rows(), (uint32_t)f->R, outdeg,
+					f->nz_outdeg.as<uint32_t>());
+			LG_CUDA(cudaGetLastError(), "pr_row_degrees");
+			s->launches++;
+		}
+		f->has_nz_outdeg = true;
 	}
 	const uint32_t ntiles = f->ntiles;
 	const uint32_t* flat_off = f->off.as<uint32_t>();
@@ -399,6 +417,7 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 	a.ids = f->ids.as<uint32_t>();
 	a.heads = f->heads();
 	a.nz_rows = f->nz_rows();
+	a.nz_outdeg = f->nz_outdeg.as<uint32_t>();
 	a.nz_off = f->nz_off();
 	a.tile_seg = f->tile_seg();
 	a.E = (uint32_t)f->E;
