@@ -15,6 +15,7 @@ e2e      = the same step through the C ABI with host buffers: every step
            re-ingests the newest level from host memory (pinned staging),
            reopens the snapshot and copies ranks and BFS levels back to host
 roofline = the PageRank iteration kernel (pr_flat_step), HBM-bound
+bfs_roofline = the BFS phase against the per-root byte model (lower bound)
 --impl reference times the reference's own OpenMP kernels (oracle/_ref, built
 from the reference source) on the host cores for the same step.
 
@@ -40,7 +41,7 @@ METRIC = "GTEPS (PageRank iter, BFS) on multiversion R-MAT; batched BC & adjoint
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="lg", choices=["lg", "reference"])
     p.add_argument("--scale", type=int, default=24)
@@ -90,16 +91,49 @@ def dist_init(args):
 
 
 class Clocks:
-    """nvidia-smi sampler for the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region: an
+    NVML thread every 10 ms (device found by its PCI bus id), else
+    nvidia-smi every 200 ms."""
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device):
         self.device = device
         self.p = None
+        self.thread = None
+        self.rows = []
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.device)
+        bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
 
     def start(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop_flag = threading.Event()
+
+            def run():
+                while not self.stop_flag.is_set():
+                    mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.rows.append((mhz, self.max_mhz) +
+                                     tuple("active" if r & b else "" for b in bits))
+                    self.stop_flag.wait(0.01)
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.p = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
@@ -109,30 +143,32 @@ class Clocks:
             self.p = None
 
     def stop(self):
-        if self.p is None:
-            return None
-        self.p.terminate()
-        out, _ = self.p.communicate(timeout=10)
-        rows = []
-        for line in out.strip().splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 8:
-                continue
-            try:
-                rows.append((float(f[0]), float(f[1]), f[4], f[5], f[6], f[7]))
-            except ValueError:
-                continue
+        rows, source = self.rows, "nvml 10 ms"
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+        elif self.p is not None:
+            source = "nvidia-smi 200 ms"
+            self.p.terminate()
+            out, _ = self.p.communicate(timeout=10)
+            for line in out.strip().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 8:
+                    continue
+                try:
+                    rows.append((float(f[0]), float(f[1]), f[4], f[5], f[6], f[7]))
+                except ValueError:
+                    continue
         if not rows:
             return None
         reasons = set()
         for r in rows:
-            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown",
-                                "sw_thermal_slowdown", "sw_power_cap"), r[2:]):
+            for name, v in zip(self.NAMES, r[2:]):
                 if v.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(r[0] for r in rows),
                 "sm_max_mhz": max(r[1] for r in rows), "samples": len(rows),
-                "reasons": sorted(reasons)}
+                "source": source, "reasons": sorted(reasons)}
 
 
 def measured_peak():
@@ -179,20 +215,27 @@ def run_reference(args):
     E = int(deg.sum())
     cores = Reference.max_threads()
 
-    def step():
-        pr, t_pr = R.pagerank_pull(-1, args.pr_iters, 0.85)
+    # each step is a quarter of the device step, in the same proportions:
+    # pr_iters/4 PageRank iterations + BFS from a quarter of the roots, the
+    # roots taken in turn so that four steps cover all of them
+    q_it = max(1, args.pr_iters // 4)
+    q_roots = max(1, len(roots) // 4)
+
+    def step(i):
+        pr, t_pr = R.pagerank_pull(-1, q_it, 0.85)
         edges, t_bfs = 0, 0.0
-        for r in roots:
+        for j in range(q_roots):
+            r = roots[(i * q_roots + j) % len(roots)]
             lv, t = R.bfs(-1, int(r))
             t_bfs += t
             edges += int(deg[lv < 2147483646].sum(dtype=np.int64))
-        return t_pr + t_bfs, args.pr_iters * E + edges
+        return t_pr + t_bfs, q_it * E + edges
 
-    for _ in range(args.warmup):
-        step()
+    for i in range(args.warmup):
+        step(i)
     tot_t, tot_e = 0.0, 0
-    for _ in range(args.steps):
-        t, e = step()
+    for i in range(args.steps):
+        t, e = step(i)
         tot_t += t
         tot_e += e
     gteps = tot_e / tot_t / 1e9
@@ -203,10 +246,10 @@ def run_reference(args):
             "config": cfg,
             "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": cores,
                              "kind": "reference",
-                             "sample": "each step = the full step (pagerank_double x"
-                                       f"{args.pr_iters} + sssp_unweighted BFS from "
-                                       f"{len(roots)} roots) on the same store, run() "
-                                       "time only"},
+                             "sample": f"each step = a quarter of the device step: "
+                                       f"pagerank_double x{q_it} + sssp_unweighted BFS "
+                                       f"from {q_roots} of the {len(roots)} roots in turn, "
+                                       "on the same store, run() time only"},
             "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     emit(line, args)
@@ -337,6 +380,23 @@ def run_lg(args):
                                   "full-size launch (profiles/pr_flat_step_rmat24.md)"
                                   if traffic else None}
 
+    # BFS of the step, against the per-root byte model of the path's survey:
+    # sum over roots of (4 B id + 4 B neighbour level per reached out-edge)
+    # + 4 B level per vertex; the 12 B per reached fragment term is left out,
+    # so the figure is a lower bound of that model. The multi-source and
+    # bottom-up steps read fewer bytes than the model charges, so this is the
+    # effective bandwidth of the BFS phase (all its kernels), not a DRAM count.
+    bfs_s = bfs_ms / args.steps / 1e3
+    bfs_bytes = 8 * reach + 4 * V * len(roots)
+    bfs_roofline = {"bound": "hbm", "kernels": "BFS phase of the step (%s-source)"
+                    % ("multi" if args.bfs == "multi" else "single"),
+                    "achieved": bfs_bytes / bfs_s / 1e9, "peak": peak, "unit": "GB/s",
+                    "frac": bfs_bytes / bfs_s / 1e9 / peak,
+                    "algorithmic_bytes_per_step": bfs_bytes,
+                    "bytes_model": "sum over roots of 8*E_reach + 4*V (fragment term "
+                                   "omitted: lower bound)",
+                    "ms_per_step": bfs_s * 1e3, "roots": len(roots)}
+
     # e2e: newest level re-ingested from host, snapshot reopened, results to host
     e2e = None
     if not args.no_e2e:
@@ -369,7 +429,7 @@ def run_lg(args):
             "graph": {"max_nodes": V, "live_edges": E, "in_slots": ins["slots"],
                       "in_fragments": ins["fragments"], "levels": hg.num_levels,
                       "host_build_s": build_s, "ingest_s": ingest_s},
-            "roofline": roofline, "e2e": e2e, "gpu_launches": launches,
+            "roofline": roofline, "bfs_roofline": bfs_roofline, "e2e": e2e, "gpu_launches": launches,
             "clocks": clk, "cpu_baseline": cpu, "extras": ext}
     if rank == 0:
         emit(line, args)
@@ -388,7 +448,7 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
     flattens its in-CSR, and copies the ranks and BFS levels to pinned host
     memory.  The same with the host-built level ingested through
     lg_store_ingest_level is reported as host_level.  Then one more step with
-    a synchronisation after each phase gives the breakdown."""
+    a synchronisation after each phase (no overlap) gives the breakdown."""
     import torch
     pr_host = torch.empty(V, dtype=torch.float64).pin_memory()
     lv_host = torch.empty((len(roots), V), dtype=torch.int32).pin_memory()
@@ -407,30 +467,49 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
         else:
             st.ingest_level(desc)
 
-    def analytics(phase=None):
+    def bfs():
+        if args.bfs == "multi":
+            _, rs = s2.bfs_multi(roots, out=lv_host)
+            return sum(r.reach_edges for r in rs)
+        reach = 0
+        for i, r in enumerate(roots):
+            _, res = s2.bfs(int(r), out=lv_host[i])
+            reach += res.reach_edges
+        return reach
+
+    s2 = None
+
+    def analytics(phase=None, overlap=True):
+        # overlap: the BFS levels (16 x 4 B per vertex) go to the host on the
+        # store's copy stream (LG_OUTPUT_ASYNC) while PageRank runs
+        nonlocal s2
         s2 = st.snapshot()
         if phase:
             phase("snapshot_open")
         s2.flatten(1)
-        s2.pagerank_pull(args.pr_iters, 0.85, out=pr_host)
-        if phase:
-            phase("flatten_pagerank_to_host")
-        reach = 0
-        if args.bfs == "multi":
-            _, rs = s2.bfs_multi(roots, out=lv_host)
-            reach = sum(r.reach_edges for r in rs)
+        if overlap:
+            st.set_output_mode("async")
+            reach = bfs()
+            if phase:
+                phase("bfs")
+            s2.pagerank_pull(args.pr_iters, 0.85, out=pr_host)
+            st.sync()                        # every result of the step is on the host
+            st.set_output_mode("sync")
+            if phase:
+                phase("pagerank_and_copies_to_host")
         else:
-            for i, r in enumerate(roots):
-                _, res = s2.bfs(int(r), out=lv_host[i])
-                reach += res.reach_edges
-        if phase:
-            phase("bfs_to_host")
+            s2.pagerank_pull(args.pr_iters, 0.85, out=pr_host)
+            if phase:
+                phase("flatten_pagerank_to_host")
+            reach = bfs()
+            if phase:
+                phase("bfs_to_host")
         s2.close()
         return reach
 
-    def measure(kind):
+    def measure(kind, overlap=True):
         load(kind)
-        analytics()
+        analytics(overlap=overlap)
         st.sync()
         barrier(ws)
         h0, d0 = st.transfer_bytes()
@@ -440,7 +519,8 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
         e0.record(stream)
         for _ in range(args.steps):
             load(kind)
-            edges += args.pr_iters * E + analytics()
+            edges += args.pr_iters * E + analytics(overlap=overlap)
+        st.sync()
         e1.record(stream)
         stream.synchronize()
         h1, d1 = st.transfer_bytes()
@@ -453,11 +533,15 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
 
     out = measure("device")
     out["includes"] = ("newest level rebuilt on the device from its edge delta (pinned host "
-                       "arrays) + snapshot open + in-CSR flatten + PageRank + BFS with "
-                       "results copied to pinned host memory")
+                       "arrays) + snapshot open + in-CSR flatten + BFS + PageRank, results "
+                       "copied to pinned host memory (BFS levels on the store's copy stream "
+                       "while PageRank runs; all on the host at the end of every step)")
     host = measure("host")
     host["includes"] = "as above, the level built on the host and ingested"
     out["host_level"] = host
+    sync = measure("device", overlap=False)
+    sync["includes"] = "as the main figure, every result copied back before the next call"
+    out["sync_output"] = sync
     # phase breakdown of one more device-built step (host clock, synchronised)
     phases = {}
     t = [time.perf_counter()]
@@ -472,7 +556,7 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
     t[0] = time.perf_counter()
     st.build_level(V, p_src, p_dst, p_w, p_dsrc, p_ddst)
     phase("build_level")
-    analytics(phase)
+    analytics(phase, overlap=False)
     out["phases_ms"] = phases
     return out
 

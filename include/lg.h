@@ -157,6 +157,25 @@ lg_status lg_store_ingest_level(lg_store* store, const lg_level_desc* level);
 int       lg_store_num_levels(const lg_store* store);
 lg_status lg_store_max_nodes(const lg_store* store, int level, uint64_t* max_nodes);
 lg_status lg_store_sync(lg_store* store);
+
+/* Host output mode of a store (no reference counterpart: the reference's
+ * kernels write host arrays in place).
+ *   LG_OUTPUT_SYNC  (default) a call with a host output buffer returns after
+ *                   the result is in that buffer.
+ *   LG_OUTPUT_ASYNC an output of at least LG_ASYNC_MIN_BYTES written to
+ *                   page-locked host memory (cudaHostAlloc / cudaHostRegister)
+ *                   is staged in a device buffer of the store and copied on a
+ *                   second stream of the store, so the copy overlaps the calls
+ *                   that follow; the buffer holds the result after
+ *                   lg_store_sync().  The caller keeps it alive and does not
+ *                   read it before then.  Pageable host memory, smaller
+ *                   outputs and the lg_*_result structs are returned as in
+ *                   LG_OUTPUT_SYNC.  Two outputs can be in flight; a third
+ *                   waits (on the device) for the oldest copy. */
+#define LG_OUTPUT_SYNC     0
+#define LG_OUTPUT_ASYNC    1
+#define LG_ASYNC_MIN_BYTES (1ull << 20)
+lg_status lg_store_set_output_mode(lg_store* store, int mode);
 /* The stream every call of this store runs on (a cudaStream_t). */
 void*     lg_store_stream(const lg_store* store);
 /* Device bytes held by the store (levels, deletions, scratch). */

@@ -27,6 +27,9 @@ LG_NIL_EDGE = -1
 LG_FRESH_MAX_LEVEL = (1 << 26) - 1
 LG_MAX_LEVELS = 64
 LG_UNREACHED = 2147483646
+LG_OUTPUT_SYNC = 0
+LG_OUTPUT_ASYNC = 1
+LG_ASYNC_MIN_BYTES = 1 << 20
 LG_GEN_RMAT = 0
 LG_GEN_KRONECKER = 1
 
@@ -126,6 +129,7 @@ SIGNATURES = [
     ("lg_store_num_levels", _INT, [_P]),
     ("lg_store_max_nodes", _INT, [_P, _INT, C.POINTER(_U64)]),
     ("lg_store_sync", _INT, [_P]),
+    ("lg_store_set_output_mode", _INT, [_P, _INT]),
     ("lg_store_stream", _P, [_P]),
     ("lg_store_device_bytes", _U64, [_P]),
     ("lg_store_launch_count", _U64, [_P]),

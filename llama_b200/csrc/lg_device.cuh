@@ -230,6 +230,14 @@ struct lg_store {
 	lg::DevLevel* level_spare[2] = {nullptr, nullptr};
 	lg::DevBuf build_tmp[12];   // lg_store_build_level temporaries
 	int min_level = 0;          // levels below are aged out (lg_store_set_min_level)
+	// LG_OUTPUT_ASYNC: results staged in out_stage[i] and copied to host on
+	// copy_stream; stage_done[i] marks the end of slot i's last copy
+	int output_mode = 0;
+	cudaStream_t copy_stream = nullptr;
+	lg::DevBuf out_stage[2];
+	cudaEvent_t stage_ready[2] = {nullptr, nullptr};
+	cudaEvent_t stage_done[2] = {nullptr, nullptr};
+	int stage_next = 0;
 };
 
 // Edge-order maps of a snapshot used by the differentiable PageRank

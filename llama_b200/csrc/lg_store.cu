@@ -58,8 +58,47 @@ bool is_device_pointer(const void* ptr) {
 	return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+static bool is_pinned_host(const void* ptr) {
+	cudaPointerAttributes a;
+	cudaError_t e = cudaPointerGetAttributes(&a, ptr);
+	if (e != cudaSuccess) { (void)cudaGetLastError(); return false; }
+	return a.type == cudaMemoryTypeHost;
+}
+
+// LG_OUTPUT_ASYNC: the result is copied into a staging slot on the store's
+// stream (so the caller may reuse `src` at once) and from there to the host
+// on copy_stream.  The slot is reused only after its previous copy ended.
+static lg_status copy_out_async(lg_store* s, void* dst, const void* src, size_t bytes) {
+	if (!s->copy_stream) {
+		LG_CUDA(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "copy stream");
+		for (int i = 0; i < 2; i++) {
+			LG_CUDA(cudaEventCreateWithFlags(&s->stage_ready[i], cudaEventDisableTiming), "event");
+			LG_CUDA(cudaEventCreateWithFlags(&s->stage_done[i], cudaEventDisableTiming), "event");
+		}
+	}
+	const int i = s->stage_next;
+	s->stage_next ^= 1;
+	DevBuf& b = s->out_stage[i];
+	if (bytes > b.bytes) {
+		// the old buffer may still be read by the slot's previous copy
+		LG_CUDA(cudaStreamSynchronize(s->copy_stream), "copy stream");
+		LG_TRY(b.reserve(bytes));
+	}
+	LG_CUDA(cudaStreamWaitEvent(s->stream, s->stage_done[i], 0), "wait for slot");
+	LG_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyDeviceToDevice, s->stream), "stage result");
+	LG_CUDA(cudaEventRecord(s->stage_ready[i], s->stream), "event");
+	LG_CUDA(cudaStreamWaitEvent(s->copy_stream, s->stage_ready[i], 0), "wait for result");
+	LG_CUDA(cudaMemcpyAsync(dst, b.p, bytes, cudaMemcpyDeviceToHost, s->copy_stream),
+			"copy result");
+	LG_CUDA(cudaEventRecord(s->stage_done[i], s->copy_stream), "event");
+	s->d2h_bytes += bytes;
+	return LG_OK;
+}
+
 lg_status copy_out(lg_store* s, void* dst, const void* src, size_t bytes) {
 	if (bytes == 0) return LG_OK;
+	if (s->output_mode == LG_OUTPUT_ASYNC && bytes >= LG_ASYNC_MIN_BYTES && is_pinned_host(dst))
+		return copy_out_async(s, dst, src, bytes);
 	if (!is_device_pointer(dst)) s->d2h_bytes += bytes;
 	LG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s->stream), "copy result");
 	return LG_OK;
@@ -688,7 +727,15 @@ lg_status lg_store_destroy(lg_store* s) {
 		return set_error(LG_ESTATE, "close all snapshots before destroying the store");
 	cudaSetDevice(s->device);
 	cudaStreamSynchronize(s->stream);
-	for (int i = 0; i < 2; i++) if (s->staged[i]) cudaEventDestroy(s->staged[i]);
+	if (s->copy_stream) {
+		cudaStreamSynchronize(s->copy_stream);
+		cudaStreamDestroy(s->copy_stream);
+	}
+	for (int i = 0; i < 2; i++) {
+		if (s->staged[i]) cudaEventDestroy(s->staged[i]);
+		if (s->stage_ready[i]) cudaEventDestroy(s->stage_ready[i]);
+		if (s->stage_done[i]) cudaEventDestroy(s->stage_done[i]);
+	}
 	if (s->pinned) cudaFreeHost(s->pinned);
 	delete s->flat_scratch;
 	for (int d = 0; d < 2; d++) {
@@ -751,7 +798,25 @@ lg_status lg_store_max_nodes(const lg_store* s, int level, uint64_t* mn) {
 lg_status lg_store_sync(lg_store* s) {
 	clear_error();
 	if (!s) return set_error(LG_EINVAL, "null store");
+	if (s->copy_stream) {
+		// the store's stream waits for the result copies, so that work
+		// queued on it after this call (an event, say) comes after them too
+		for (int i = 0; i < 2; i++)
+			LG_CUDA(cudaStreamWaitEvent(s->stream, s->stage_done[i], 0), "join copies");
+		LG_CUDA(cudaStreamSynchronize(s->copy_stream), "sync copies");
+	}
 	LG_CUDA(cudaStreamSynchronize(s->stream), "sync");
+	return LG_OK;
+}
+
+lg_status lg_store_set_output_mode(lg_store* s, int mode) {
+	clear_error();
+	if (!s) return set_error(LG_EINVAL, "null store");
+	if (mode != LG_OUTPUT_SYNC && mode != LG_OUTPUT_ASYNC)
+		return set_error(LG_EINVAL, "unknown output mode %d", mode);
+	if (mode == LG_OUTPUT_SYNC && s->copy_stream)
+		LG_CUDA(cudaStreamSynchronize(s->copy_stream), "sync copies");
+	s->output_mode = mode;
 	return LG_OK;
 }
 

@@ -172,6 +172,13 @@ class Store:
     def sync(self):
         check(lib.lg_store_sync(self._h))
 
+    def set_output_mode(self, mode):
+        """"sync" (default) or "async": with "async", results of 1 MiB or more
+        written to page-locked host tensors are copied on a second stream and
+        are in place after sync() (lg_store_set_output_mode)."""
+        m = {"sync": _lib.LG_OUTPUT_SYNC, "async": _lib.LG_OUTPUT_ASYNC}.get(mode, mode)
+        check(lib.lg_store_set_output_mode(self._h, int(m)))
+
     @property
     def launch_count(self):
         return lib.lg_store_launch_count(self._h)
