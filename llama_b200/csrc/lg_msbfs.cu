@@ -216,41 +216,90 @@ ms_bottom_up(SnapCsr in, u64 lanes, const u64* cur, const u64* seen, u64* nxt) {
 // get level depth + 1; the vertex joins the next queue.  ctr[0] next queue
 // length, ctr[1] its out-degree sum, ctr[2] OR of the new bits.
 //
-// The level rows are written root by root for all threads of a warp alike,
-// so the lanes holding bit k write row k at consecutive vertices together.
-__global__ void ms_commit(const uint32_t* list, uint32_t n, uint32_t depth1, uint64_t V,
+// A CTA takes kCommitPer rounds of kMsThreads consecutive entries.  The
+// level rows are written root by root for all threads of a warp alike, so
+// the lanes holding bit k write row k at consecutive vertices together.
+// The queue slots and the counters are taken once per CTA (a dense step
+// commits every vertex, and one atomic per warp on the same three counters
+// serialised in L2).
+constexpr int kCommitPer = 4;
+__global__ void __launch_bounds__(kMsThreads)
+ms_commit(const uint32_t* list, uint32_t n, uint32_t depth1, uint64_t V,
 		int nroots, u64* nxt, u64* seen, u64* cur2, int32_t* levels, const uint32_t* outdeg,
 		uint32_t* queue, unsigned long long* ctr) {
-	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	uint32_t w = 0;
-	u64 bits = 0;
-	if (i < n) {
-		w = list ? __ldg(list + i) : (uint32_t)i;
-		const u64 c = nxt[w];
-		if (c) {
-			nxt[w] = 0;
-			bits = c & ~seen[w];
-			if (bits) {
-				seen[w] |= bits;
-				cur2[w] = bits;
+	constexpr int kWarps = kMsThreads / 32;
+	__shared__ uint32_t s_cnt[kWarps];
+	__shared__ unsigned long long s_e[kWarps];
+	__shared__ u64 s_any[kWarps];
+	__shared__ unsigned long long s_base;
+	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+	const uint64_t b0 = (uint64_t)blockIdx.x * (kMsThreads * kCommitPer) + threadIdx.x;
+	uint32_t ws[kCommitPer];
+	unsigned masks[kCommitPer];
+	uint32_t cnt = 0;
+	unsigned long long e = 0;
+	u64 any = 0;
+#pragma unroll
+	for (int r = 0; r < kCommitPer; r++) {
+		const uint64_t i = b0 + (uint64_t)r * kMsThreads;
+		uint32_t w = 0;
+		u64 bits = 0;
+		if (i < n) {
+			w = list ? __ldg(list + i) : (uint32_t)i;
+			const u64 c = nxt[w];
+			if (c) {
+				nxt[w] = 0;
+				bits = c & ~seen[w];
+				if (bits) {
+					seen[w] |= bits;
+					cur2[w] = bits;
+				}
 			}
 		}
+		const unsigned m = __ballot_sync(0xffffffffu, bits != 0);
+		if (levels && m) {
+			for (int k = 0; k < nroots; k++)
+				if ((bits >> k) & 1ull) levels[(uint64_t)k * V + w] = (int32_t)depth1;
+		}
+		ws[r] = w;
+		masks[r] = m;
+		cnt += __popc(m);
+		if (bits) e += __ldg(outdeg + w);
+		any |= bits;
 	}
-	if (levels && __any_sync(0xffffffffu, bits != 0)) {
-		for (int k = 0; k < nroots; k++)
-			if ((bits >> k) & 1ull) levels[(uint64_t)k * V + w] = (int32_t)depth1;
-	}
-	ms_push(bits != 0, w, queue, ctr);
-	unsigned long long e = bits ? __ldg(outdeg + w) : 0ull;
-	u64 any = bits;
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1) {
 		e += __shfl_xor_sync(0xffffffffu, e, o);
 		any |= __shfl_xor_sync(0xffffffffu, any, o);
 	}
-	if ((threadIdx.x & 31u) == 0) {
-		if (e) atomicAdd(ctr + 1, e);
-		if (any) atomicOr(ctr + 2, any);
+	if (lane == 0) {
+		s_cnt[wid] = cnt;
+		s_e[wid] = e;
+		s_any[wid] = any;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		uint32_t tot = 0;
+		unsigned long long et = 0;
+		u64 at = 0;
+		for (int x = 0; x < kWarps; x++) {
+			const uint32_t c = s_cnt[x];
+			s_cnt[x] = tot;
+			tot += c;
+			et += s_e[x];
+			at |= s_any[x];
+		}
+		s_base = tot ? atomicAdd(ctr, (unsigned long long)tot) : 0ull;
+		if (et) atomicAdd(ctr + 1, et);
+		if (at) atomicOr(ctr + 2, at);
+	}
+	__syncthreads();
+	unsigned long long pos = s_base + s_cnt[wid];
+#pragma unroll
+	for (int r = 0; r < kCommitPer; r++) {
+		const unsigned m = masks[r];
+		if ((m >> lane) & 1u) queue[pos + __popc(m & ((1u << lane) - 1u))] = ws[r];
+		pos += __popc(m);
 	}
 }
 
@@ -583,7 +632,8 @@ extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int 
 				LG_CUDA(cudaMemcpyAsync(&nc, ctr + 3, sizeof(nc), cudaMemcpyDeviceToHost, st), "d2h");
 				LG_CUDA(cudaStreamSynchronize(st), "bc batched");
 				if (nc > 0)
-					ms_commit<<<grid_for(nc, B), B, 0, st>>>(cand, (uint32_t)nc, k + 1, V, n, nxt,
+					ms_commit<<<grid_for(nc, kMsThreads * kCommitPer), kMsThreads, 0, st>>>(cand,
+							(uint32_t)nc, k + 1, V, n, nxt,
 							seen, lk1, nullptr, outdeg, q2, ctr);
 				s->launches += 5 + (nc > 0);
 			} else {
@@ -597,7 +647,8 @@ extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int 
 				} else
 					ms_bottom_up<<<grid_for(V, kMsThreads), kMsThreads, 0, st>>>(in, lanes, lk,
 							seen, nxt);
-				ms_commit<<<grid_for(V, B), B, 0, st>>>(nullptr, (uint32_t)V, k + 1, V, n, nxt,
+				ms_commit<<<grid_for(V, kMsThreads * kCommitPer), kMsThreads, 0, st>>>(nullptr,
+						(uint32_t)V, k + 1, V, n, nxt,
 						seen, lk1, nullptr, outdeg, q2, ctr);
 				s->launches += 5;
 			}
@@ -741,7 +792,8 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 				LG_CUDA(cudaMemcpyAsync(&nc, ctr + 3, sizeof(nc), cudaMemcpyDeviceToHost, st), "d2h");
 				LG_CUDA(cudaStreamSynchronize(st), "msbfs step");
 				if (nc > 0)
-					ms_commit<<<grid_for(nc, B), B, 0, st>>>(cand, (uint32_t)nc, depth + 1, V, n, nxt,
+					ms_commit<<<grid_for(nc, kMsThreads * kCommitPer), kMsThreads, 0, st>>>(cand,
+							(uint32_t)nc, depth + 1, V, n, nxt,
 							seen, cur2, plv, outdeg, q2, ctr);
 				td++;
 				s->launches += 5 + (nc > 0);
@@ -756,7 +808,8 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 				} else
 					ms_bottom_up<<<grid_for(V, kMsThreads), kMsThreads, 0, st>>>(in, lanes, cur,
 							seen, nxt);
-				ms_commit<<<grid_for(V, B), B, 0, st>>>(nullptr, (uint32_t)V, depth + 1, V, n, nxt,
+				ms_commit<<<grid_for(V, kMsThreads * kCommitPer), kMsThreads, 0, st>>>(nullptr,
+						(uint32_t)V, depth + 1, V, n, nxt,
 						seen, cur2, plv, outdeg, q2, ctr);
 				bu++;
 				s->launches += 2;
