@@ -17,6 +17,7 @@ namespace lg {
 constexpr int32_t kUnreached = LG_UNREACHED;
 constexpr int kBfsThreads = 256;
 constexpr uint32_t kBfsRange = 1024;
+constexpr uint64_t kBfsWarps = 148ull * 64;   // about the warps a B200 holds at once
 constexpr int kBuChunk = 4;            // in-neighbours a bottom-up round checks
 constexpr int kBuVerts = 4;            // vertices a flat bottom-up thread interleaves
 
@@ -51,6 +52,55 @@ __device__ __forceinline__ void warp_add_u64(unsigned long long x,
 	if ((threadIdx.x & 31) == 0 && x) atomicAdd(dst, x);
 }
 
+// Block-aggregated append for the dense steps, which visit every vertex:
+// each thread offers N items (take[j], item[j]) and adds `sum` to len[1];
+// the block takes its queue slots with one atomic on len[0] and adds its
+// sum with one more, instead of two atomics per warp on the same counters.
+// Every thread of the block (kBfsThreads) calls it.
+template <int N>
+__device__ __forceinline__ void block_append(const bool (&take)[N], const uint32_t (&item)[N],
+		unsigned long long sum, uint32_t* queue, unsigned long long* len) {
+	constexpr int kWarps = kBfsThreads / 32;
+	__shared__ uint32_t s_cnt[kWarps];
+	__shared__ unsigned long long s_sum[kWarps];
+	__shared__ unsigned long long s_base;
+	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+	unsigned m[N];
+	uint32_t cnt = 0;
+#pragma unroll
+	for (int j = 0; j < N; j++) {
+		m[j] = __ballot_sync(0xffffffffu, take[j]);
+		cnt += __popc(m[j]);
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+	if (lane == 0) {
+		s_cnt[wid] = cnt;
+		s_sum[wid] = sum;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		uint32_t tot = 0;
+		unsigned long long st = 0;
+		for (int x = 0; x < kWarps; x++) {
+			const uint32_t c = s_cnt[x];
+			s_cnt[x] = tot;
+			tot += c;
+			st += s_sum[x];
+		}
+		s_base = tot ? atomicAdd(len, (unsigned long long)tot) : 0ull;
+		if (st) atomicAdd(len + 1, st);
+	}
+	__syncthreads();
+	unsigned long long pos = s_base + s_cnt[wid];
+	const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+	for (int j = 0; j < N; j++) {
+		if (take[j]) queue[pos + __popc(m[j] & below)] = item[j];
+		pos += __popc(m[j]);
+	}
+}
+
 // Fragment slots of every frontier entry (to be scanned into range offsets).
 __global__ void bfs_frontier_slots(SnapCsr out, const uint32_t* queue, uint32_t qlen,
 		uint32_t* cnt) {
@@ -60,20 +110,20 @@ __global__ void bfs_frontier_slots(SnapCsr out, const uint32_t* queue, uint32_t 
 	cnt[i] = vertex_slots(out, __ldg(queue + i), &f0);
 }
 
-// Top-down step over the frontier's slot space cut into kBfsRange-slot
-// ranges, one warp each (lg_expand.cuh).  ctr[0] = next frontier size,
+// Top-down step over the frontier's slot space cut into ranges of at most
+// kBfsRange slots, one warp each (lg_expand.cuh).  ctr[0] = next frontier size,
 // ctr[1] = sum of out-degrees of the next frontier.
 __global__ void __launch_bounds__(kBfsThreads)
 bfs_top_down(SnapCsr out, const uint32_t* queue, const uint32_t* fpos, uint32_t qlen,
-		uint32_t total, uint32_t nranges, int32_t* level, uint32_t* next,
+		uint32_t total, uint32_t range, uint32_t nranges, int32_t* level, uint32_t* next,
 		unsigned long long* ctr, int32_t cur) {
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint64_t r64 = (uint64_t)blockIdx.x * (kBfsThreads / 32) + (threadIdx.x >> 5);
 	if (r64 >= nranges) return;
 	const uint32_t r = (uint32_t)r64;
 	const bool last_range = r == nranges - 1;
-	const uint32_t ra = r * kBfsRange;
-	const uint32_t rb = last_range ? total : min(total, ra + kBfsRange);
+	const uint32_t ra = r * range;
+	const uint32_t rb = last_range ? total : min(total, ra + range);
 	uint32_t e_begin, e_end;
 	range_entries(fpos, qlen, ra, rb, last_range, &e_begin, &e_end);
 	const LevelTab* lt = out.lt;
@@ -151,8 +201,9 @@ bfs_bottom_up(SnapCsr in, const uint32_t* outdeg, const uint32_t* bits,
 		}
 		if (found) level[v] = cur + 1;
 	}
-	warp_append(found, v, next, ctr);
-	warp_add_u64(found ? __ldg(outdeg + v) : 0ull, ctr + 1);
+	const bool take[1] = {found};
+	const uint32_t item[1] = {v};
+	block_append(take, item, found ? __ldg(outdeg + v) : 0ull, next, ctr);
 }
 
 // Bottom-up step over a flat in-CSR (lg_snapshot_flatten).  A thread takes
@@ -198,13 +249,14 @@ bfs_bottom_up_flat(const uint32_t* off, const uint32_t* ids, uint32_t V,
 		}
 	}
 	unsigned long long mf = 0;
+	uint32_t item[kBuVerts];
 #pragma unroll
 	for (int j = 0; j < kBuVerts; j++) {
 		const uint32_t v = base + j * kBfsThreads;
+		item[j] = v;
 		if (found[j]) { level[v] = cur + 1; mf += __ldg(outdeg + v); }
-		warp_append(found[j], v, next, ctr);
 	}
-	warp_add_u64(mf, ctr + 1);
+	block_append(found, item, mf, next, ctr);
 }
 
 } // namespace lg
@@ -267,17 +319,21 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 			top_down = true;
 		LG_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st), "memset");
 		if (top_down) {
-			// frontier slot offsets, then one warp per kBfsRange slots
+			// frontier slot offsets, then one warp per range
 			bfs_frontier_slots<<<grid_for(qlen, 256), 256, 0, st>>>(out, q,
 					(uint32_t)qlen, fcnt);
 			uint64_t total = 0;
 			LG_TRY(exclusive_scan_u32(fcnt, fpos, qlen, sc[7], st, &total));
 			s->d2h_bytes += 8;
-			const uint32_t nranges = (uint32_t)((total + kBfsRange - 1) / kBfsRange);
+			// ranges of up to kBfsRange slots, shorter (down to 32) when the
+			// frontier is too small to give every resident warp one
+			uint64_t range = (total + kBfsWarps - 1) / kBfsWarps;
+			range = std::min<uint64_t>(std::max<uint64_t>((range + 31) & ~31ull, 32), kBfsRange);
+			const uint32_t nranges = (uint32_t)((total + range - 1) / range);
 			if (nranges > 0)
 				bfs_top_down<<<grid_for(nranges, kBfsThreads / 32), kBfsThreads, 0, st>>>(
-						out, q, fpos, (uint32_t)qlen, (uint32_t)total, nranges, lvl, nq,
-						ctr, cur);
+						out, q, fpos, (uint32_t)qlen, (uint32_t)total, (uint32_t)range, nranges,
+						lvl, nq, ctr, cur);
 			td_steps++;
 			s->launches += 5;
 		} else {

@@ -29,7 +29,16 @@ namespace lg {
 typedef unsigned long long u64;
 constexpr int32_t kMsUnreached = LG_UNREACHED;
 constexpr int kMsThreads = 256;
-constexpr uint32_t kMsRange = 1024;
+constexpr uint32_t kMsRange = 1024;     // largest slot range per warp
+
+// Slots per warp range for a list of `total` slots over `nwarps` warps: the
+// even share rounded up to 32, between 32 and kMsRange, so a small frontier
+// is spread over many warps instead of a few long ones.
+__device__ __forceinline__ uint32_t ms_range(uint32_t total, uint32_t nwarps) {
+	uint32_t r = (uint32_t)(((uint64_t)total + nwarps - 1) / nwarps);
+	r = (r + 31u) & ~31u;
+	return min(max(r, 32u), kMsRange);
+}
 constexpr int kMsChunk = 4;            // in-neighbours per bottom-up round
 constexpr int kMsMaxRoots = 64;        // roots per pass
 
@@ -74,11 +83,12 @@ __global__ void __launch_bounds__(kMsThreads)
 ms_top_down(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
 		const u64* cur, const u64* seen, u64* nxt, uint32_t* cand, unsigned long long* ncand) {
 	const uint32_t total = __ldg(pos + qlen);
-	const uint32_t nranges = (total + kMsRange - 1) / kMsRange;
 	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	const uint32_t range = ms_range(total, nwarps);
+	const uint32_t nranges = (total + range - 1) / range;
 	for (uint32_t r = warp; r < nranges; r += nwarps) {
-		range_for_each(out, queue, pos, qlen, total, nranges, kMsRange, r,
+		range_for_each(out, queue, pos, qlen, total, nranges, range, r,
 			[&](bool act, uint32_t, uint32_t ov, uint32_t nbr, uint32_t, uint32_t) {
 				bool first = false;
 				if (act) {
@@ -388,11 +398,12 @@ bcm_sigma(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen
 		const u64* lk, const u64* lk1, double* sigma) {
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint32_t total = __ldg(pos + qlen);
-	const uint32_t nranges = (total + kMsRange - 1) / kMsRange;
 	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	const uint32_t range = ms_range(total, nwarps);
+	const uint32_t nranges = (total + range - 1) / range;
 	for (uint32_t r = warp; r < nranges; r += nwarps) {
-		range_for_each(out, queue, pos, qlen, total, nranges, kMsRange, r,
+		range_for_each(out, queue, pos, qlen, total, nranges, range, r,
 			[&](bool act, uint32_t, uint32_t v, uint32_t w, uint32_t, uint32_t) {
 				const u64 m = act ? (__ldg(lk + v) & __ldg(lk1 + w)) : 0ull;
 				unsigned todo = __ballot_sync(0xffffffffu, m != 0);
@@ -423,13 +434,14 @@ bcm_delta(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen
 		const u64* lk, const u64* lk1, const double* sigma, double* delta) {
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint32_t total = __ldg(pos + qlen);
-	const uint32_t nranges = (total + kMsRange - 1) / kMsRange;
 	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	const uint32_t range = ms_range(total, nwarps);
+	const uint32_t nranges = (total + range - 1) / range;
 	for (uint32_t r = warp; r < nranges; r += nwarps) {
 		uint32_t cur = 0xffffffffu;
 		double a0 = 0.0, a1 = 0.0;
-		range_for_each(out, queue, pos, qlen, total, nranges, kMsRange, r,
+		range_for_each(out, queue, pos, qlen, total, nranges, range, r,
 			[&](bool act, uint32_t, uint32_t v, uint32_t w, uint32_t, uint32_t) {
 				const u64 m = act ? (__ldg(lk + v) & __ldg(lk1 + w)) : 0ull;
 				unsigned todo = __ballot_sync(0xffffffffu, m != 0);
