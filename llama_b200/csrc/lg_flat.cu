@@ -3,11 +3,11 @@
 // Reference: ll_t_flatten (benchmark/tools/flatten.h) merges every level of
 // a LLAMA graph into a single level by iterating each vertex's edges
 // (newest fragment first, deleted edges skipped) on the host.  Here the
-// same order is produced in two balanced passes over the virtual slot space
-// (one CTA per 1024 virtual slots): flat_count counts each block's live
-// slots, a scan turns the counts into block bases, and flat_write writes
-// every live slot's id (and weight) at its block base + live rank, and every
-// vertex's row start.  Row bookkeeping for the tile kernels (heads, nz_rows,
+// same order is produced in one balanced pass over the virtual slot space
+// (one CTA per 1024 virtual slots): row starts are the scan of the live
+// degrees, and flat_write writes every live slot's id (and weight) at its
+// block's base (found from the row start of the block's first vertex) + its
+// live rank.  Row bookkeeping for the tile kernels (heads, nz_rows,
 // nz_off, tile_seg) and the optional fragment view follow.
 #include "lg_flat.cuh"
 
@@ -16,46 +16,50 @@
 
 namespace lg {
 
-// blk_live[r] = live slots of block r.
+// Writes the live slots of block r to ids[base ...] in slot order (and their
+// weights to w when non-null).  base = the live slots before the block:
+// off[e] of the entry e that holds the block's first slot, plus e's live
+// slots before it (its deleted slots counted a word at a time).  off is the
+// exclusive scan of the snapshot's live degrees; every entry that starts in
+// the block checks it against its rank in the block, and a mismatch (a
+// degree that is not the live slot count) sets bit 2 of *err.
 __global__ void __launch_bounds__(kMapThreads)
-flat_count(SlotSpace sp, uint32_t* blk_live) {
-	__shared__ BlockMap m;
-	__shared__ uint32_t red[kMapThreads / 32];
-	const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
-	const uint32_t r = blockIdx.x, ra = r * kMapRange, rb = block_end(sp, r);
-	map_block(sp, r, ra, rb, m);
-	uint32_t c = 0;
-#pragma unroll
-	for (int u = 0; u < kMapPerThread; u++) {
-		uint32_t lv, idx;
-		if (block_slot(m, ra, rb, u * kMapThreads + tid, &lv, &idx))
-			c += !slot_deleted(sp.g.lt, lv, idx);
-	}
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-	if (lane == 0) red[wid] = c;
-	__syncthreads();
-	if (tid == 0) {
-		uint32_t t = 0;
-		for (int w = 0; w < kMapThreads / 32; w++) t += red[w];
-		blk_live[r] = t;
-	}
-}
-
-// Writes the live slots of block r to ids[blk_base[r] ...] (and their
-// weights to w when non-null) in slot order, and off[e] for every entry e
-// that starts in the block (off has V + 1 entries; the last block also
-// writes the trailing ones).
-__global__ void __launch_bounds__(kMapThreads)
-flat_write(SlotSpace sp, const uint32_t* blk_base, uint32_t* ids, uint32_t* w,
-		uint32_t* off) {
+flat_write(SlotSpace sp, const uint32_t* off, uint32_t E, uint32_t* ids, uint32_t* w,
+		unsigned int* err) {
 	constexpr int kGroups = kMapPerThread * (kMapThreads / 32);
 	__shared__ BlockMap m;
 	__shared__ uint16_t rank[kMapRange];
 	__shared__ uint32_t gpre[kGroups];
+	__shared__ uint32_t dead_w[kMapThreads / 32];
 	const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
 	const uint32_t r = blockIdx.x, ra = r * kMapRange, rb = block_end(sp, r);
 	map_block(sp, r, ra, rb, m);
+
+	// the first entry's slots before ra: its fragments lead ftab
+	const uint32_t e0 = m.eb;
+	uint32_t before = 0, dead = 0;
+	if (m.nf > 0 && m.fstart[0] < ra) {
+		const uint32_t nfe = min(__ldg(sp.g.frag_off + e0 + 1) - __ldg(sp.g.frag_off + e0), m.nf);
+		for (uint32_t i = 0; i < nfe; i++) {
+			const uint32_t s0 = m.fstart[i];
+			if (s0 >= ra) break;
+			const uint2 fr = m.ftab[i];
+			const uint32_t n = min(frag_len(fr), ra - s0);
+			before += n;
+			const uint32_t* d = sp.g.lt->del[frag_level(fr)];
+			const uint32_t a = fr.x, b = fr.x + n;          // slots [a, b)
+			for (uint32_t wd = (a >> 5) + tid; wd <= ((b - 1) >> 5); wd += kMapThreads) {
+				uint32_t x = __ldg(d + wd);
+				if (wd == (a >> 5)) x &= ~0u << (a & 31);
+				if (wd == ((b - 1) >> 5) && (b & 31)) x &= (1u << (b & 31)) - 1u;
+				dead += __popc(x);
+			}
+		}
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) dead += __shfl_xor_sync(0xffffffffu, dead, o);
+	if (lane == 0) dead_w[wid] = dead;
+
 	uint32_t id[kMapPerThread], wt[kMapPerThread], mask[kMapPerThread];
 #pragma unroll
 	for (int u = 0; u < kMapPerThread; u++) {
@@ -84,7 +88,10 @@ flat_write(SlotSpace sp, const uint32_t* blk_base, uint32_t* ids, uint32_t* w,
 		if (lane < (uint32_t)kGroups) gpre[lane] = x - c;
 	}
 	__syncthreads();
-	const uint32_t base = __ldg(blk_base + r);
+	uint32_t dead_all = 0;
+#pragma unroll
+	for (int x = 0; x < kMapThreads / 32; x++) dead_all += dead_w[x];
+	const uint32_t base = __ldg(off + e0) + before - dead_all;
 	const uint32_t below = (1u << lane) - 1u;
 #pragma unroll
 	for (int u = 0; u < kMapPerThread; u++) {
@@ -92,20 +99,29 @@ flat_write(SlotSpace sp, const uint32_t* blk_base, uint32_t* ids, uint32_t* w,
 		const uint32_t rk = gpre[u * (kMapThreads / 32) + wid] + __popc(mask[u] & below);
 		rank[k] = (uint16_t)rk;
 		if ((mask[u] >> lane) & 1u) {
-			ids[base + rk] = id[u];
-			if (w) w[base + rk] = wt[u];
+			if (base + rk < E) {
+				ids[base + rk] = id[u];
+				if (w) w[base + rk] = wt[u];
+			} else {
+				atomicOr(err, 2u);      // degrees and live slots disagree
+			}
 		}
 	}
 	__syncthreads();
-	const uint32_t V = (uint32_t)sp.g.V;
-	const bool last = r == sp.nranges - 1;
+	// entries starting in the block: their row start must be base + rank
 	const uint32_t e_begin = __ldg(sp.range_lb + r);
-	const uint32_t e_end = last ? V + 1 : __ldg(sp.range_lb + r + 1);
-	const uint32_t next = __ldg(blk_base + r + 1);
+	const uint32_t e_end = r == sp.nranges - 1 ? (uint32_t)sp.g.V : __ldg(sp.range_lb + r + 1);
+	bool bad = false;
 	for (uint32_t e = e_begin + tid; e < e_end; e += kMapThreads) {
 		const uint32_t p = __ldg(sp.pos + e);
-		off[e] = p < rb ? base + rank[p - ra] : next;
+		if (p < rb && p >= ra) bad |= __ldg(off + e) != base + rank[p - ra];
 	}
+	if (r == sp.nranges - 1 && tid == kMapThreads - 1) {
+		// the last block ends at the total of the degrees
+		const uint32_t nlive = gpre[kGroups - 1] + __popc(mask[kMapPerThread - 1]);
+		bad |= base + nlive != __ldg(off + sp.g.V);
+	}
+	if (bad) atomicOr(err, 2u);
 }
 
 __global__ void flat_flags(const uint32_t* off, uint64_t V, uint32_t* flags) {
@@ -178,13 +194,9 @@ lg_status build_flat(lg_snapshot* sn, int dir, FlatCsr& f, bool view) {
 	f.V = V;
 	f.has_view = false;
 	f.has_nz_outdeg = false;
-	LG_TRY(f.blk.reserve(2ull * (sp.nranges + 1) * sizeof(uint32_t)));
-	uint32_t* blk_live = f.blk.as<uint32_t>();
-	uint32_t* blk_base = blk_live + sp.nranges + 1;
-	flat_count<<<sp.nranges, kMapThreads, 0, st>>>(sp, blk_live);
-	LG_CUDA(cudaGetLastError(), "flat_count");
-	uint64_t E = 0;
-	LG_TRY(exclusive_scan_u32(blk_live, blk_base, sp.nranges, f.scan_tmp, st, &E));
+	// row starts from the live degrees; flat_write checks them
+	const SnapDir& d = dir == 0 ? sn->out : sn->in;
+	const uint64_t E = d.n_edges;
 	if (E > 0xffffffffull - 2 * kFlatTile)
 		return set_error(LG_ENOTSUP, "more than 2^32 - %u live edges in one direction",
 				2 * kFlatTile);
@@ -195,16 +207,24 @@ lg_status build_flat(lg_snapshot* sn, int dir, FlatCsr& f, bool view) {
 	if (weighted) LG_TRY(f.w.reserve(std::max<uint64_t>(E, 1) * sizeof(uint32_t)));
 	LG_TRY(f.off.reserve((V + 1) * sizeof(uint32_t)));
 	LG_TRY(f.kidx.reserve((V + 1) * sizeof(uint32_t)));
+	LG_TRY(f.err.reserve(sizeof(unsigned int)));
 	uint32_t* off = f.off.as<uint32_t>();
-	flat_write<<<sp.nranges, kMapThreads, 0, st>>>(sp, blk_base, f.ids.as<uint32_t>(),
-			weighted ? f.w.as<uint32_t>() : nullptr, off);
+	LG_CUDA(cudaMemsetAsync(f.err.p, 0, sizeof(unsigned int), st), "clear flag");
+	LG_TRY(exclusive_scan_u32(d.deg.as<uint32_t>(), off, V, f.scan_tmp, st, nullptr));
+	flat_write<<<sp.nranges, kMapThreads, 0, st>>>(sp, off, (uint32_t)E, f.ids.as<uint32_t>(),
+			weighted ? f.w.as<uint32_t>() : nullptr, f.err.as<unsigned int>());
 	LG_CUDA(cudaGetLastError(), "flat_write");
+	unsigned int err = 0;
+	LG_CUDA(cudaMemcpyAsync(&err, f.err.p, sizeof(err), cudaMemcpyDeviceToHost, st), "d2h");
 	LG_TRY(f.flags.reserve(std::max<uint64_t>(V, 1) * sizeof(uint32_t)));
 	flat_flags<<<grid_for(V, B), B, 0, st>>>(off, V, f.flags.as<uint32_t>());
 	LG_CUDA(cudaGetLastError(), "flat_flags");
 	uint64_t R = 0;
 	LG_TRY(exclusive_scan_u32(f.flags.as<uint32_t>(), f.kidx.as<uint32_t>(), V, f.scan_tmp,
 			st, &R));
+	// (the scan waited for the stream, so err is in)
+	if (err & 2u)
+		return set_error(LG_EINVAL, "a vertex's degree differs from its live edge count");
 	f.R = R;
 	const uint64_t head_words = (uint64_t)f.ntiles * kFlatTileWords + 1;
 	LG_TRY(f.rows.reserve((2 * f.rcap() + f.ntiles + head_words) * sizeof(uint32_t)));
@@ -218,13 +238,12 @@ lg_status build_flat(lg_snapshot* sn, int dir, FlatCsr& f, bool view) {
 				const_cast<uint32_t*>(f.tile_seg()));
 		LG_CUDA(cudaGetLastError(), "flat_tiles");
 	}
-	s->launches += 2 + 3 + 1 + 3 + 1 + (f.ntiles > 0);
+	s->launches += 3 + 1 + 1 + 3 + 1 + (f.ntiles > 0);
 	if (!view) return LG_OK;
 
 	LG_TRY(f.vfrags.reserve(f.rcap() * sizeof(uint2)));
 	const uint64_t del_words = (E + 31) / 32 + 1;
 	LG_TRY(f.vdel.reserve(del_words * sizeof(uint32_t)));
-	LG_TRY(f.err.reserve(sizeof(unsigned int)));
 	LG_CUDA(cudaMemsetAsync(f.vdel.p, 0, del_words * sizeof(uint32_t), st), "clear view bits");
 	LG_CUDA(cudaMemsetAsync(f.err.p, 0, sizeof(unsigned int), st), "clear flag");
 	if (R > 0) {
@@ -240,7 +259,6 @@ lg_status build_flat(lg_snapshot* sn, int dir, FlatCsr& f, bool view) {
 	lt.w[0] = weighted ? f.w.as<uint32_t>() : nullptr;
 	LG_TRY(f.vlt.reserve(sizeof(LevelTab)));
 	LG_CUDA(cudaMemcpyAsync(f.vlt.p, &lt, sizeof(lt), cudaMemcpyHostToDevice, st), "level table");
-	unsigned int err = 0;
 	LG_CUDA(cudaMemcpyAsync(&err, f.err.p, sizeof(err), cudaMemcpyDeviceToHost, st), "d2h");
 	LG_CUDA(cudaStreamSynchronize(st), "flatten");
 	if (err)

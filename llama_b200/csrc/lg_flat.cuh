@@ -169,7 +169,7 @@ struct FlatCsr {
 	DevBuf ids;                // E u32
 	DevBuf w;                  // E u32 (weighted)
 	DevBuf rows;               // nz_rows[R] nz_off[R] tile_seg[ntiles] heads[ntiles*8+1]
-	DevBuf blk, flags, scan_tmp, err;   // build scratch
+	DevBuf flags, scan_tmp, err;        // build scratch
 	DevBuf vfrags, vdel, vlt;  // one-fragment-per-vertex view
 	DevBuf nz_outdeg;          // R u32: out-degree of each row (PageRank, built on use)
 	bool has_nz_outdeg = false;
