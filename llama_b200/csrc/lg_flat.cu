@@ -35,6 +35,21 @@ flat_write(SlotSpace sp, const uint32_t* off, uint32_t E, uint32_t* ids, uint32_
 	const uint32_t r = blockIdx.x, ra = r * kMapRange, rb = block_end(sp, r);
 	map_block(sp, r, ra, rb, m);
 
+	// the block's slots: deletion word, id (and weight) loads issued first,
+	// for every slot, so they overlap the count below
+	uint32_t dw[kMapPerThread], id[kMapPerThread], wt[kMapPerThread], mask[kMapPerThread];
+	uint32_t bit[kMapPerThread];
+	bool have[kMapPerThread];
+#pragma unroll
+	for (int u = 0; u < kMapPerThread; u++) {
+		uint32_t lv = 0, idx = 0;
+		have[u] = block_slot(m, ra, rb, u * kMapThreads + tid, &lv, &idx);
+		dw[u] = have[u] ? __ldg(sp.g.lt->del[lv] + (idx >> 5)) : 0u;
+		id[u] = have[u] ? __ldg(sp.g.lt->ids[lv] + idx) : 0u;
+		wt[u] = (have[u] && w) ? __ldg(sp.g.lt->w[lv] + idx) : 0u;
+		bit[u] = idx & 31u;
+	}
+
 	// the first entry's slots before ra: its fragments lead ftab
 	const uint32_t e0 = m.eb;
 	uint32_t before = 0, dead = 0;
@@ -60,16 +75,9 @@ flat_write(SlotSpace sp, const uint32_t* off, uint32_t E, uint32_t* ids, uint32_
 	for (int o = 16; o > 0; o >>= 1) dead += __shfl_xor_sync(0xffffffffu, dead, o);
 	if (lane == 0) dead_w[wid] = dead;
 
-	uint32_t id[kMapPerThread], wt[kMapPerThread], mask[kMapPerThread];
 #pragma unroll
-	for (int u = 0; u < kMapPerThread; u++) {
-		uint32_t lv = 0, idx = 0;
-		bool live = block_slot(m, ra, rb, u * kMapThreads + tid, &lv, &idx);
-		if (live) live = !slot_deleted(sp.g.lt, lv, idx);
-		id[u] = live ? __ldg(sp.g.lt->ids[lv] + idx) : 0u;
-		wt[u] = (live && w) ? __ldg(sp.g.lt->w[lv] + idx) : 0u;
-		mask[u] = __ballot_sync(0xffffffffu, live);
-	}
+	for (int u = 0; u < kMapPerThread; u++)
+		mask[u] = __ballot_sync(0xffffffffu, have[u] && !((dw[u] >> bit[u]) & 1u));
 	// slot order is k = u * kMapThreads + wid * 32 + lane: group u * 4 + wid
 	if (lane == 0) {
 #pragma unroll

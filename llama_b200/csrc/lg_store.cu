@@ -195,25 +195,47 @@ __global__ void scan_sums_single(uint64_t* sums, uint64_t n, uint64_t* grand) {
 	if (threadIdx.x == 0) *grand = carry;
 }
 
+// A thread scans kScanItems consecutive values; with 16-byte aligned arrays
+// it moves them as two 16-byte vectors each way.
 __global__ void scan_tiles(const uint32_t* in, uint32_t* out, uint64_t n,
 		const uint64_t* sums, const uint64_t* grand) {
+	static_assert(kScanItems == 8, "two 16-byte vectors per thread");
 	uint64_t base = (uint64_t)blockIdx.x * kScanTile
 		+ (uint64_t)threadIdx.x * kScanItems;
+	const bool vec = ((((uintptr_t)in) | ((uintptr_t)out)) & 15u) == 0 && base + kScanItems <= n;
 	uint32_t vals[kScanItems];
+	if (vec) {
+		const uint4 a = __ldcs(reinterpret_cast<const uint4*>(in + base));
+		const uint4 b = __ldcs(reinterpret_cast<const uint4*>(in + base + 4));
+		vals[0] = a.x; vals[1] = a.y; vals[2] = a.z; vals[3] = a.w;
+		vals[4] = b.x; vals[5] = b.y; vals[6] = b.z; vals[7] = b.w;
+	} else {
+#pragma unroll
+		for (int i = 0; i < kScanItems; i++) {
+			uint64_t idx = base + i;
+			vals[i] = idx < n ? in[idx] : 0;
+		}
+	}
 	uint64_t s = 0;
 #pragma unroll
-	for (int i = 0; i < kScanItems; i++) {
-		uint64_t idx = base + i;
-		vals[i] = idx < n ? in[idx] : 0;
-		s += vals[i];
-	}
+	for (int i = 0; i < kScanItems; i++) s += vals[i];
 	uint64_t tot;
 	uint64_t ex = block_excl_scan(s, &tot) + sums[blockIdx.x];
+	uint32_t o[kScanItems];
 #pragma unroll
 	for (int i = 0; i < kScanItems; i++) {
-		uint64_t idx = base + i;
-		if (idx < n) out[idx] = (uint32_t)ex;
+		o[i] = (uint32_t)ex;
 		ex += vals[i];
+	}
+	if (vec) {
+		reinterpret_cast<uint4*>(out + base)[0] = make_uint4(o[0], o[1], o[2], o[3]);
+		reinterpret_cast<uint4*>(out + base)[1] = make_uint4(o[4], o[5], o[6], o[7]);
+	} else {
+#pragma unroll
+		for (int i = 0; i < kScanItems; i++) {
+			uint64_t idx = base + i;
+			if (idx < n) out[idx] = o[i];
+		}
 	}
 	if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = (uint32_t)*grand;
 }
