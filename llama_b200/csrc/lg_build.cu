@@ -351,14 +351,6 @@ static lg_status sorted_keys(lg_store* s, const uint32_t* a, const uint32_t* b, 
 	return LG_OK;
 }
 
-// Appends deletion marks to a direction's list (host mirror + device copy).
-static lg_status append_marks(lg_store* s, DevCsr& csr, const std::vector<uint2>& add) {
-	const size_t old_n = csr.dels_host.size();
-	csr.dels_mark.push_back(old_n);
-	csr.dels_host.insert(csr.dels_host.end(), add.begin(), add.end());
-	return upload_dels(s, csr, old_n);
-}
-
 } // namespace lg
 
 using namespace lg;
@@ -408,7 +400,6 @@ extern "C" lg_status lg_store_build_level(lg_store* s, uint64_t max_nodes,
 			ok_perm, sc + 4, &ok, &operm));
 	LG_TRY(sorted_keys(s, xs, xd, n_del, V, false, kErrDupDel, err, od_keys, ok_perm,
 			sc + 4, &od, nullptr));
-	std::vector<uint2> out_marks(n_del), in_marks;
 	DevBuf& marks = s->build_tmp[9];
 	LG_TRY(marks.reserve(std::max<uint64_t>(2 * n_del, 1) * sizeof(uint2)));
 	if (l > 0) {
@@ -475,17 +466,9 @@ extern "C" lg_status lg_store_build_level(lg_store* s, uint64_t max_nodes,
 	unsigned herr = 0;
 	if (!rs) {
 		cudaError_t ce = cudaMemcpyAsync(&herr, err, sizeof(herr), cudaMemcpyDeviceToHost, st);
-		if (ce == cudaSuccess && n_del > 0)
-			ce = cudaMemcpyAsync(out_marks.data(), marks.p, n_del * sizeof(uint2),
-					cudaMemcpyDeviceToHost, st);
-		if (ce == cudaSuccess && s->reverse && n_del > 0) {
-			in_marks.resize(n_del);
-			ce = cudaMemcpyAsync(in_marks.data(), marks.as<uint2>() + n_del, n_del * sizeof(uint2),
-					cudaMemcpyDeviceToHost, st);
-		}
 		if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
 		if (ce != cudaSuccess) rs = cuda_status(ce, "build level");
-		s->d2h_bytes += sizeof(herr) + (s->reverse ? 2 : 1) * n_del * sizeof(uint2);
+		s->d2h_bytes += sizeof(herr);
 	}
 	if (!rs && herr) {
 		if (herr & kErrRange) rs = set_error(LG_EINVAL, "vertex id out of range");
@@ -502,10 +485,11 @@ extern "C" lg_status lg_store_build_level(lg_store* s, uint64_t max_nodes,
 	}
 	// commit
 	s->out.levels.push_back(lo);
-	LG_TRY(append_marks(s, s->out, out_marks));
+	// the deletion marks go from the build buffer to the lists, on the device
+	LG_TRY(append_dels(s, s->out, marks.as<uint2>(), n_del, cudaMemcpyDeviceToDevice));
 	if (s->reverse) {
 		s->in.levels.push_back(li);
-		LG_TRY(append_marks(s, s->in, in_marks));
+		LG_TRY(append_dels(s, s->in, marks.as<uint2>() + n_del, n_del, cudaMemcpyDeviceToDevice));
 	}
 	LG_CUDA(cudaStreamSynchronize(st), "build level");
 	return LG_OK;

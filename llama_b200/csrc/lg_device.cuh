@@ -162,10 +162,11 @@ struct DevLevel {
 
 struct DevCsr {
 	std::vector<DevLevel*> levels;
-	std::vector<uint2> dels_host;   // (index, level << 26 | max_visible_level)
-	std::vector<size_t> dels_mark;  // dels_host.size() before each level's ingest
-	DevBuf dels;                    // device copy of dels_host
-	uint64_t n_dels_dev = 0;
+	// deletion marks (index, level << 26 | max_visible_level) of all levels,
+	// in level order, on the device only
+	DevBuf dels;
+	uint64_t n_dels_dev = 0;        // marks in dels
+	std::vector<size_t> dels_mark;  // n_dels_dev before each level's marks
 	~DevCsr() { for (DevLevel* l : levels) delete l; }
 };
 
@@ -285,9 +286,10 @@ lg_status copy_out(lg_store* s, void* dst, const void* src, size_t bytes);
 // allocation fails.
 DevLevel* take_level(lg_store* s, int dir);
 
-// Brings the device deletion list of csr up to its host mirror, whose first
-// old_n entries the device copy already holds.
-lg_status upload_dels(lg_store* s, DevCsr& csr, size_t old_n);
+// Appends a level's n deletion marks (host or device memory, per kind) to
+// csr's device list and records where the level's marks begin.
+lg_status append_dels(lg_store* s, DevCsr& csr, const uint2* add, size_t n,
+		cudaMemcpyKind kind);
 
 inline unsigned grid_for(uint64_t n, unsigned block) {
 	uint64_t g = (n + block - 1) / block;

@@ -112,25 +112,29 @@ DevLevel* take_level(lg_store* s, int dir) {
 	return d;
 }
 
-lg_status upload_dels(lg_store* s, DevCsr& csr, size_t old_n) {
-	const size_t n = csr.dels_host.size();
-	if (n == 0) { csr.n_dels_dev = 0; return LG_OK; }
-	const size_t need = n * sizeof(uint2);
-	size_t from = std::min(old_n, csr.n_dels_dev);
+lg_status append_dels(lg_store* s, DevCsr& csr, const uint2* add, size_t n,
+		cudaMemcpyKind kind) {
+	const size_t old_n = csr.n_dels_dev;
+	const size_t need = (old_n + n) * sizeof(uint2);
 	if (need > csr.dels.bytes) {
-		// the previous device copy may still be read by queued kernels
+		// a larger list keeps the marks already on the device
+		DevBuf nb;
+		LG_TRY(nb.reserve(need + need / 2));
+		if (old_n)
+			LG_CUDA(cudaMemcpyAsync(nb.p, csr.dels.p, old_n * sizeof(uint2),
+					cudaMemcpyDeviceToDevice, s->stream), "deletion list");
+		// the old list may still be read by queued kernels
 		LG_CUDA(cudaStreamSynchronize(s->stream), "deletion list");
-		LG_TRY(csr.dels.reserve(need + need / 2));
-		from = 0;
+		csr.dels.swap(nb);
 	}
-	if (n > from) {
-		// pageable source: the copy completes before cudaMemcpyAsync returns
-		LG_CUDA(cudaMemcpyAsync(csr.dels.as<uint2>() + from, csr.dels_host.data() + from,
-				(n - from) * sizeof(uint2), cudaMemcpyHostToDevice, s->stream),
-				"deletion list");
-		s->h2d_bytes += (n - from) * sizeof(uint2);
+	if (n) {
+		// (a pageable host source is copied before cudaMemcpyAsync returns)
+		LG_CUDA(cudaMemcpyAsync(csr.dels.as<uint2>() + old_n, add, n * sizeof(uint2), kind,
+				s->stream), "deletion list");
+		if (kind == cudaMemcpyHostToDevice) s->h2d_bytes += n * sizeof(uint2);
 	}
-	csr.n_dels_dev = n;
+	csr.dels_mark.push_back(old_n);
+	csr.n_dels_dev = old_n + n;
 	return LG_OK;
 }
 
@@ -423,11 +427,8 @@ static lg_status ingest_csr(lg_store* s, DevCsr& csr, int l,
 		}
 		add.push_back(make_uint2((uint32_t)ix, (el << LG_BITS_LEVEL) | x.max_visible_level));
 	}
-	const size_t old_n = csr.dels_host.size();
-	csr.dels_mark.push_back(old_n);
 	csr.levels.push_back(d);
-	csr.dels_host.insert(csr.dels_host.end(), add.begin(), add.end());
-	return upload_dels(s, csr, old_n);
+	return append_dels(s, csr, add.data(), add.size(), cudaMemcpyHostToDevice);
 }
 
 // ---------------------------------------------------------------------------
@@ -881,10 +882,9 @@ lg_status lg_store_drop_level(lg_store* s) {
 		delete s->level_spare[dir];               // keep the newest dropped level's buffers
 		s->level_spare[dir] = c->levels.back();
 		c->levels.pop_back();
-		// the device copy keeps the same prefix of the list
-		c->dels_host.resize(c->dels_mark.back());
+		// the list keeps the marks of the levels below
+		c->n_dels_dev = c->dels_mark.back();
 		c->dels_mark.pop_back();
-		c->n_dels_dev = c->dels_host.size();
 	}
 	return LG_OK;
 }
