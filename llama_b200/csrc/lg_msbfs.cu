@@ -318,41 +318,46 @@ __global__ void ms_clear(const uint32_t* queue, uint32_t n, u64* cur) {
 	if (i < n) cur[__ldg(queue + i)] = 0;
 }
 
-// Per-root reached vertices and the out-degree sum over them.  A warp takes
-// 32 vertices at a time and, for every root k, counts the lanes holding bit
-// k (ballot) and adds their out-degrees (warp reductions of the two 16-bit
-// halves, so no sum can overflow); lane k keeps root k's running totals
-// (lane k - 32 for roots 32..63) and adds them to the global counters once.
-__global__ void ms_reach(const u64* seen, const uint32_t* outdeg, uint64_t V, int n,
+// Per-root reached vertices and the out-degree sum over them, from the level
+// rows: CTA column y takes root y's row (4 levels and 4 out-degrees per
+// 16-byte load when the rows are aligned) and adds its block totals once.
+// The out-degree array is read once per root, mostly from L2.
+__global__ void ms_reach(const int32_t* levels, const uint32_t* outdeg, uint64_t V,
 		unsigned long long* cnt, unsigned long long* edges) {
-	const uint32_t lane = threadIdx.x & 31u;
-	const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-	unsigned long long c0 = 0, c1 = 0, e0 = 0, e1 = 0;   // roots lane, lane + 32
-	for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
-		const uint64_t v = base + lane;
-		const u64 b = v < V ? seen[v] : 0ull;
-		if (!__any_sync(0xffffffffu, b != 0)) continue;
-		const uint32_t d = v < V ? __ldg(outdeg + v) : 0u;
-		for (int k = 0; k < n; k++) {
-			const bool has = (b >> k) & 1ull;
-			const uint32_t c = __popc(__ballot_sync(0xffffffffu, has));
-			if (!c) continue;
-			const uint32_t lo = __reduce_add_sync(0xffffffffu, has ? (d & 0xffffu) : 0u);
-			const uint32_t hi = __reduce_add_sync(0xffffffffu, has ? (d >> 16) : 0u);
-			const unsigned long long e = (unsigned long long)lo + ((unsigned long long)hi << 16);
-			if ((uint32_t)(k & 31) == lane) {
-				if (k < 32) { c0 += c; e0 += e; } else { c1 += c; e1 += e; }
-			}
+	__shared__ unsigned long long sc[8], se[8];
+	const int k = blockIdx.y;
+	const int32_t* row = levels + (uint64_t)k * V;
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	uint64_t c = 0, e = 0;
+	const bool vec = ((((uintptr_t)row) | ((uintptr_t)outdeg)) & 15u) == 0;
+	uint64_t v0 = 0;
+	if (vec) {
+		const uint64_t nq = V / 4;
+		for (uint64_t q = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += stride) {
+			const int4 l = __ldcs(reinterpret_cast<const int4*>(row) + q);
+			const uint4 d = __ldg(reinterpret_cast<const uint4*>(outdeg) + q);
+			if (l.x != kMsUnreached) { c++; e += d.x; }
+			if (l.y != kMsUnreached) { c++; e += d.y; }
+			if (l.z != kMsUnreached) { c++; e += d.z; }
+			if (l.w != kMsUnreached) { c++; e += d.w; }
 		}
+		v0 = nq * 4;
 	}
-	if ((int)lane < n) {
-		if (c0) atomicAdd(cnt + lane, c0);
-		if (e0) atomicAdd(edges + lane, e0);
+	for (uint64_t v = v0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += stride)
+		if (row[v] != kMsUnreached) { c++; e += __ldg(outdeg + v); }
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		c += __shfl_xor_sync(0xffffffffu, c, o);
+		e += __shfl_xor_sync(0xffffffffu, e, o);
 	}
-	if ((int)lane + 32 < n) {
-		if (c1) atomicAdd(cnt + lane + 32, c1);
-		if (e1) atomicAdd(edges + lane + 32, e1);
+	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+	if (lane == 0) { sc[wid] = c; se[wid] = e; }
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		unsigned long long tc = 0, te = 0;
+		for (uint32_t x = 0; x < (blockDim.x >> 5); x++) { tc += sc[x]; te += se[x]; }
+		if (tc) atomicAdd(cnt + k, tc);
+		if (te) atomicAdd(edges + k, te);
 	}
 }
 
@@ -841,7 +846,8 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 			std::swap(cur, cur2);
 		}
 		if (results) {
-			ms_reach<<<(unsigned)sms * 4u, B, 0, st>>>(seen, outdeg, V, n, lane_cnt, lane_edges);
+			ms_reach<<<dim3((unsigned)sms * 2u, (unsigned)n), B, 0, st>>>(plv, outdeg, V,
+					lane_cnt, lane_edges);
 			LG_CUDA(cudaGetLastError(), "ms_reach");
 			s->launches++;
 			std::vector<unsigned long long> hc(2 * kMsMaxRoots);
