@@ -598,12 +598,17 @@ def extras(args, st, stream, device):
             roots = workloads.pick_roots(sn.out_degrees(), 8, seed=13)
             dist = torch.empty(V, dtype=torch.int32, device=dev)
             sn.sssp(int(roots[0]), 32, out=dist)
-            reach, ms = 0, 0.0
+            reach, ms, rounds, buckets, relax = 0, 0.0, 0, 0, 0
             for r in roots:
                 (_, rr), t = _timed(stream, lambda: sn.sssp(int(r), 32, out=dist))
                 reach += rr.reach_edges
                 ms += t
-            res["sssp_delta32_8roots"] = {"ms": ms, "gteps": reach / (ms / 1e3) / 1e9}
+                rounds += rr.rounds
+                buckets += rr.buckets
+                relax += rr.relaxations
+            res["sssp_delta32_8roots"] = {"ms": ms, "gteps": reach / (ms / 1e3) / 1e9,
+                                          "rounds": rounds, "buckets": buckets,
+                                          "relaxations_per_reached_edge": relax / max(reach, 1)}
             sn.triangle_count()
             tc, ms = _timed(stream, sn.triangle_count)
             res["triangle_count"] = {"ms": ms, "triangles": tc.triangles,

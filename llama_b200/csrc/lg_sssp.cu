@@ -32,16 +32,33 @@ __global__ void sssp_init(uint32_t* dist, uint32_t* stamp, uint32_t* fstamp,
 	if (v == 0) queue[0] = root;
 }
 
-__device__ __forceinline__ void warp_push(bool take, uint32_t item,
-		uint32_t* queue, unsigned long long* len) {
-	unsigned m = __ballot_sync(0xffffffffu, take);
-	if (!m) return;
+// Per-warp staging of queue appends in shared memory: items collect in a
+// kPushBuf-entry buffer and go to the global queue kPushBuf at a time with
+// one atomic, instead of one atomic on the same counter per 32 items (which
+// serialises in L2 when most warps append).  n is warp-uniform.
+constexpr uint32_t kPushBuf = 128;
+
+__device__ __forceinline__ void wq_flush(uint32_t* sbuf, uint32_t& n, uint32_t* queue,
+		unsigned long long* len) {
+	if (n == 0) return;
 	const uint32_t lane = threadIdx.x & 31u;
-	const int leader = __ffs(m) - 1;
+	__syncwarp();
 	unsigned long long base = 0;
-	if ((int)lane == leader) base = atomicAdd(len, (unsigned long long)__popc(m));
-	base = __shfl_sync(0xffffffffu, base, leader);
-	if (take) queue[base + __popc(m & ((1u << lane) - 1u))] = item;
+	if (lane == 0) base = atomicAdd(len, (unsigned long long)n);
+	base = __shfl_sync(0xffffffffu, base, 0);
+	for (uint32_t i = lane; i < n; i += 32u) queue[base + i] = sbuf[i];
+	__syncwarp();
+	n = 0;
+}
+
+__device__ __forceinline__ void wq_add(bool take, uint32_t item, uint32_t* sbuf, uint32_t& n,
+		uint32_t* queue, unsigned long long* len) {
+	const unsigned m = __ballot_sync(0xffffffffu, take);
+	if (!m) return;
+	if (n + (uint32_t)__popc(m) > kPushBuf) wq_flush(sbuf, n, queue, len);
+	const uint32_t lane = threadIdx.x & 31u;
+	if (take) sbuf[n + __popc(m & ((1u << lane) - 1u))] = item;
+	n += __popc(m);
 }
 
 // One relaxation round over the near queue.  The queue's slot space
@@ -54,12 +71,14 @@ __global__ void __launch_bounds__(kSsspThreads)
 sssp_relax(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
 		uint32_t* dist, uint32_t* stamp, uint32_t* fstamp, uint32_t round, uint32_t epoch,
 		uint32_t hi, uint32_t* near_next, uint32_t* far, unsigned long long* ctr) {
-	const uint32_t lane = threadIdx.x & 31u;
+	__shared__ uint32_t sbuf[kSsspThreads / 32][2][kPushBuf];
+	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
 	const uint32_t total = __ldg(pos + qlen);
 	const uint32_t nranges = (total + kSsspRange - 1) / kSsspRange;
 	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
 	unsigned long long relax = 0;
+	uint32_t nn = 0, nf = 0;       // staged near / far appends of this warp
 	for (uint32_t r = warp; r < nranges; r += nwarps) {
 		range_for_each(out, queue, pos, qlen, total, nranges, kSsspRange, r,
 			[&](bool act, uint32_t, uint32_t ov, uint32_t nbr, uint32_t lv, uint32_t idx) {
@@ -75,10 +94,12 @@ sssp_relax(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qle
 						}
 					}
 				}
-				warp_push(to_near, nbr, near_next, ctr);
-				warp_push(to_far, nbr, far, ctr + 1);
+				wq_add(to_near, nbr, sbuf[wid][0], nn, near_next, ctr);
+				wq_add(to_far, nbr, sbuf[wid][1], nf, far, ctr + 1);
 			});
 	}
+	wq_flush(sbuf[wid][0], nn, near_next, ctr);
+	wq_flush(sbuf[wid][1], nf, far, ctr + 1);
 	for (int o = 16; o > 0; o >>= 1) relax += __shfl_down_sync(0xffffffffu, relax, o);
 	if (lane == 0 && relax) atomicAdd(ctr + 2, relax);
 }
@@ -87,20 +108,31 @@ sssp_relax(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qle
 // near queue (entries below lo were settled from a near queue after they
 // entered the pile), entries >= hi are kept, stamped with the new epoch, and
 // the smallest kept distance is reported in ctr[2].
-__global__ void sssp_split_far(const uint32_t* far, unsigned long long n,
+__global__ void __launch_bounds__(kSsspThreads)
+sssp_split_far(const uint32_t* far, unsigned long long n,
 		const uint32_t* dist, uint32_t* stamp, uint32_t* fstamp, uint32_t round,
 		uint32_t epoch, uint32_t lo, uint32_t hi, uint32_t* near, uint32_t* keep,
 		unsigned long long* ctr) {
-	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	uint32_t v = 0, d = kInf;
-	if (i < n) { v = far[i]; d = __ldcg(dist + v); }
-	const bool near_take = i < n && d >= lo && d < hi
-		&& atomicExch(stamp + v, round) != round;
-	const bool keep_take = i < n && d >= hi && d < kInf
-		&& atomicExch(fstamp + v, epoch) != epoch;
-	warp_push(near_take, v, near, ctr);
-	warp_push(keep_take, v, keep, ctr + 1);
-	unsigned long long m = keep_take ? d : ~0ull;
+	__shared__ uint32_t sbuf[kSsspThreads / 32][2][kPushBuf];
+	const uint32_t wid = threadIdx.x >> 5;
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	uint32_t nn = 0, nk = 0;
+	unsigned long long m = ~0ull;
+	// whole warps loop together (the bound is rounded up to the stride)
+	const uint64_t end = (n + 31) & ~31ull;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+		uint32_t v = 0, d = kInf;
+		if (i < n) { v = far[i]; d = __ldcg(dist + v); }
+		const bool near_take = i < n && d >= lo && d < hi
+			&& atomicExch(stamp + v, round) != round;
+		const bool keep_take = i < n && d >= hi && d < kInf
+			&& atomicExch(fstamp + v, epoch) != epoch;
+		wq_add(near_take, v, sbuf[wid][0], nn, near, ctr);
+		wq_add(keep_take, v, sbuf[wid][1], nk, keep, ctr + 1);
+		if (keep_take) m = min(m, (unsigned long long)d);
+	}
+	wq_flush(sbuf[wid][0], nn, near, ctr);
+	wq_flush(sbuf[wid][1], nk, keep, ctr + 1);
 	for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_down_sync(0xffffffffu, m, o));
 	if ((threadIdx.x & 31) == 0 && m != ~0ull) atomicMin(ctr + 2, m);
 }
@@ -188,7 +220,9 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 				unsigned long long init[3] = {0, 0, ~0ull};
 				LG_CUDA(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st), "h2d");
 				s->h2d_bytes += sizeof(init);
-				sssp_split_far<<<grid_for(flen, 256), 256, 0, st>>>(far, flen, d, stamp,
+				const unsigned split_blocks = (unsigned)std::min<uint64_t>(
+						std::max<uint64_t>(grid_for(flen, kSsspThreads), 1), relax_blocks);
+				sssp_split_far<<<split_blocks, kSsspThreads, 0, st>>>(far, flen, d, stamp,
 						fstamp, round, epoch, lo, hi, q, far2, ctr);
 				LG_CUDA(cudaGetLastError(), "sssp_split_far");
 				s->launches++;
