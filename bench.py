@@ -609,6 +609,17 @@ def extras(args, st, stream, device):
             res["sssp_delta32_8roots"] = {"ms": ms, "gteps": reach / (ms / 1e3) / 1e9,
                                           "rounds": rounds, "buckets": buckets,
                                           "relaxations_per_reached_edge": relax / max(reach, 1)}
+            # the same roots on the snapshot with its out-CSR flattened once
+            _, fms = _timed(stream, lambda: sn.flatten(0))
+            reach, ms = 0, 0.0
+            for r in roots:
+                (_, rr), t = _timed(stream, lambda: sn.sssp(int(r), 32, out=dist))
+                reach += rr.reach_edges
+                ms += t
+            sn.unflatten()
+            res["sssp_delta32_8roots_flat"] = {"ms": ms, "gteps": reach / (ms / 1e3) / 1e9,
+                                               "flatten_out_csr_ms": fms,
+                                               "includes": "not the one flatten"}
             sn.triangle_count()
             tc, ms = _timed(stream, sn.triangle_count)
             res["triangle_count"] = {"ms": ms, "triangles": tc.triangles,

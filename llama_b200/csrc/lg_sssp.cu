@@ -13,7 +13,10 @@
 // atomicMin on 32-bit distances, so the result does not depend on thread
 // order.  Per-vertex stamps keep every vertex at most once in the near queue
 // of a round and at most once in the far pile, which bounds both by V.
+// After lg_snapshot_flatten(snap, 0) the rounds read the flat out-CSR (ids
+// and weights in one array each, no deletion bits) instead of the levels.
 #include "lg_expand.cuh"
+#include "lg_flat.cuh"
 
 namespace lg {
 
@@ -198,7 +201,10 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 	uint32_t* stamp = sc[5].as<uint32_t>();
 	uint32_t* fstamp = stamp + V;
 	unsigned long long* ctr = sc[6].as<unsigned long long>();
-	const SnapCsr out = sn->view(0);
+	// the one-fragment view of a flattened out-CSR when there is one
+	const FlatCsr* fo = sn->flat[0];
+	const SnapCsr out = (fo && fo->has_view && fo->weighted)
+			? fo->view(sn->out.deg.as<uint32_t>()) : sn->view(0);
 
 	sssp_init<<<grid_for(V, 256), 256, 0, st>>>(d, stamp, fstamp, V, (uint32_t)root, q);
 	LG_CUDA(cudaGetLastError(), "sssp_init");

@@ -169,11 +169,14 @@ def test_golden_sssp(golden):
     with st:
         for l in range(len(golden["levels"])):
             with st.snapshot(l) as sn:
-                for i, r in enumerate(golden["roots"]):
-                    for delta in (1, 32, 1 << 20):
-                        d, res = sn.sssp(int(r), delta)
-                        assert np.array_equal(d, golden[f"sssp{l}"][i]), (l, r, delta)
-                    assert res.reached == int(np.sum(d < lb._lib.LG_UNREACHED))
+                for flat in (False, True):
+                    if flat:
+                        sn.flatten(0)           # rounds over the flat out-CSR
+                    for i, r in enumerate(golden["roots"]):
+                        for delta in (1, 32, 1 << 20):
+                            d, res = sn.sssp(int(r), delta)
+                            assert np.array_equal(d, golden[f"sssp{l}"][i]), (l, r, delta, flat)
+                        assert res.reached == int(np.sum(d < lb._lib.LG_UNREACHED))
 
 
 def test_sssp_multiversion_weights_vs_oracle():
@@ -186,11 +189,15 @@ def test_sssp_multiversion_weights_vs_oracle():
     with Store() as st:
         st.ingest(hg)
         with st.snapshot() as sn:
-            for r in workloads.pick_roots(sn.out_degrees(), 3, seed=8):
-                d, res = sn.sssp(int(r), 32)
-                ref, reached = O.sssp(3, int(r))
-                assert np.array_equal(d, ref)
-                assert res.reached == reached
+            roots = workloads.pick_roots(sn.out_degrees(), 3, seed=8)
+            for flat in (False, True):
+                if flat:
+                    sn.flatten(0)
+                for r in roots:
+                    d, res = sn.sssp(int(r), 32)
+                    ref, reached = O.sssp(3, int(r))
+                    assert np.array_equal(d, ref), (r, flat)
+                    assert res.reached == reached
 
 
 def test_sssp_needs_weights():
