@@ -320,6 +320,18 @@ lg_status lg_snapshot_is_flat(const lg_snapshot* snap, int dir, int* flat);
 lg_status lg_pagerank_pull(lg_snapshot* snap, int iterations, double damping,
 		double* ranks);
 
+/* PageRank, push direction, FP64: task "pagerank_double_push",
+ * ll_b_pagerank_push_ext<Graph,double>::run (benchmark/benchmarks/pagerank.h:258-318).
+ * Every vertex t with out-degree > 0 adds pr[t] / out_degree(t) to each
+ * out-neighbour's next value (an atomic add, as in the reference), then
+ * pr'[t] = (1-d)/N + d * next[t].  Reads only the out-CSR, so it also runs on
+ * stores kept without reverse edges.  The summation order follows the atomic
+ * schedule: results agree with lg_pagerank_pull within FP64 rounding, not bit
+ * for bit.  Uses the flat out-CSR after lg_snapshot_flatten(snap, 0).
+ * ranks: double[max_nodes]. */
+lg_status lg_pagerank_push(lg_snapshot* snap, int iterations, double damping,
+		double* ranks);
+
 /* The same PageRank for callers that cannot let the library allocate device
  * memory (this entry point has no counterpart in the reference).
  * lg_pagerank_pull grows store-owned scratch with cudaMalloc; a thread that is

@@ -154,6 +154,7 @@ SIGNATURES = [
     ("lg_snapshot_unflatten", _INT, [_P]),
     ("lg_snapshot_is_flat", _INT, [_P, _INT, C.POINTER(_INT)]),
     ("lg_pagerank_pull", _INT, [_P, _INT, _D, _P]),
+    ("lg_pagerank_push", _INT, [_P, _INT, _D, _P]),
     ("lg_pagerank_pull_noalloc", _INT, [_P, _INT, _D, _P]),
     ("lg_bfs", _INT, [_P, _I64, _P, C.POINTER(lg_bfs_result)]),
     ("lg_bfs_multi", _INT, [_P, _P, _INT, _P, _P]),

@@ -12,7 +12,8 @@
 // run() returns (benchmark.cc:1140-1154, 2019-2021).
 //
 // Options follow the reference's letters where they exist:
-//   -r TASK     pagerank_double | pagerank | bfs_count | sssp_unweighted |
+//   -r TASK     pagerank_double | pagerank | pagerank_double_push |
+//               bfs_count | sssp_unweighted |
 //               sssp_weighted | tc_u | tarjan_scc | bc_random | ppr
 //   -R ROOT     root vertex (default 0)
 //   -n N        iterations (PageRank, PPR; default 10)
@@ -97,8 +98,8 @@ void usage() {
 	fprintf(stderr,
 		"Usage: lg_benchmark [-r TASK] [-R ROOT] [-n ITERS] [-l LEVELS] [-c COUNT]\n"
 		"                    [-o FILE] [-k K] [-s SEED] [-d DEV] (-G rmat:S:L:SEED | FILE...)\n"
-		"Tasks: pagerank_double pagerank bfs_count sssp_unweighted sssp_weighted\n"
-		"       tc_u tarjan_scc bc_random ppr\n");
+		"Tasks: pagerank_double pagerank pagerank_double_push bfs_count sssp_unweighted\n"
+		"       sssp_weighted tc_u tarjan_scc bc_random ppr\n");
 }
 
 template <class T>
@@ -198,6 +199,13 @@ int main(int argc, char** argv) {
 		if (task == "pagerank_double" || task == "pagerank") {
 			std::vector<double> pr(V);
 			CHECK(lg_pagerank_pull(snap, iters, 0.85, pr.data()), "lg_pagerank_pull");
+			double s = 0;
+			for (double x : pr) s += x;
+			ret = s;
+			if (of && run == count - 1) print_part(of, pr.data(), V, "%0.6lf");
+		} else if (task == "pagerank_double_push") {
+			std::vector<double> pr(V);
+			CHECK(lg_pagerank_push(snap, iters, 0.85, pr.data()), "lg_pagerank_push");
 			double s = 0;
 			for (double x : pr) s += x;
 			ret = s;

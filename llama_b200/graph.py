@@ -367,6 +367,12 @@ class Snapshot:
         check(lib.lg_pagerank_pull(self._h, int(iterations), float(damping), ptr(res)))
         return res
 
+    def pagerank_push(self, iterations=10, damping=0.85, out=None):
+        """Task ``pagerank_double_push``: FP64 push PageRank over the out-CSR."""
+        res = np.empty(self.max_nodes, np.float64) if out is None else out
+        check(lib.lg_pagerank_push(self._h, int(iterations), float(damping), ptr(res)))
+        return res
+
     def bfs(self, root, out=None):
         """Task ``sssp_unweighted`` (BFS levels); returns (levels, lg_bfs_result)."""
         res = np.empty(self.max_nodes, np.int32) if out is None else out

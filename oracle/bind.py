@@ -44,6 +44,7 @@ def lgo():
             ("lgo_adjacency", _U64, [_P, _INT, _INT, _P, _P, _P]),
             ("lgo_degrees", None, [_P, _INT, _INT, _P]),
             ("lgo_pagerank_pull", None, [_P, _INT, _INT, _D, _P]),
+            ("lgo_pagerank_push", None, [_P, _INT, _INT, _D, _P]),
             ("lgo_bfs", _U64, [_P, _INT, _I64, _P]),
             ("lgo_bc", None, [_P, _INT, _P, _INT, _P]),
             ("lgo_sssp", _U64, [_P, _INT, _I64, _P]),
@@ -81,6 +82,7 @@ def ref():
             ("llref_set_threads", None, [_INT]),
             ("llref_max_threads", _INT, []),
             ("llref_pagerank", _D, [_P, _INT, _INT, _D, _P]),
+            ("llref_pagerank_push", _D, [_P, _INT, _INT, _D, _P]),
             ("llref_bfs_levels", _D, [_P, _INT, _I64, _P]),
             ("llref_bfs_count", _D, [_P, _INT, _I64, C.POINTER(_D)]),
             ("llref_add_level_weighted", _INT, [_P, _P, _P, _U64, _P, _P, _U64, _P]),
@@ -156,6 +158,11 @@ class Oracle(_Base):
     def pagerank_pull(self, level, iterations, damping=0.85):
         out = np.empty(self.V, np.float64)
         lgo().lgo_pagerank_pull(self.h, level, iterations, damping, _p(out))
+        return out
+
+    def pagerank_push(self, level, iterations, damping=0.85):
+        out = np.empty(self.V, np.float64)
+        lgo().lgo_pagerank_push(self.h, level, iterations, damping, _p(out))
         return out
 
     def bfs(self, level, root):
@@ -299,6 +306,11 @@ class Reference(_Base):
     def pagerank_pull(self, level, iterations, damping=0.85):
         out = np.empty(self.V, np.float64)
         secs = ref().llref_pagerank(self.h, level, iterations, damping, _p(out))
+        return out, secs
+
+    def pagerank_push(self, level, iterations, damping=0.85):
+        out = np.empty(self.V, np.float64)
+        secs = ref().llref_pagerank_push(self.h, level, iterations, damping, _p(out))
         return out, secs
 
     def bfs(self, level, root):

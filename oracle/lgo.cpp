@@ -383,6 +383,33 @@ void lgo_pagerank_pull(void* gp, int level, int max, double d, double* rank) {
 	} while (cnt < max);
 }
 
+// PageRank push, FP64: ll_b_pagerank_push_ext::run, pagerank.h:258-318.
+// Sequential here: vertices in id order, out-edges in iteration order (the
+// reference adds with an atomic in whatever order its threads run).
+void lgo_pagerank_push(void* gp, int level, int max, double d, double* rank) {
+	Graph* g = (Graph*)gp;
+	const uint64_t V = g->V;
+	const double N = (double)V;
+	std::vector<double> nxt(V, 0.0);
+	for (uint64_t t = 0; t < V; t++) rank[t] = 1 / N;
+	std::vector<uint32_t> nb;
+	const std::vector<uint32_t> od = degrees_of(g->out, level, V);
+	int cnt = 0;
+	do {
+		for (uint64_t t = 0; t < V; t++) {
+			if (od[t] == 0) continue;
+			const double delta = rank[t] / od[t];
+			neighbours(g->out, level, t, nb, nullptr);
+			for (uint32_t w : nb) nxt[w] += delta;
+		}
+		for (uint64_t t = 0; t < V; t++) {
+			rank[t] = (1 - d) / N + d * nxt[t];
+			nxt[t] = 0.0;
+		}
+		cnt = cnt + 1;
+	} while (cnt < max);
+}
+
 // Average teen count: ll_b_avg_teen_cnt::run, avg_teen_cnt.h:96-139.  For
 // every vertex n, teen_cnt[n] = in-neighbours t with 10 <= age[t] < 20; over
 // the vertices with age[n] > K, sum the counts (int32 in the reference; here

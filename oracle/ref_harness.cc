@@ -47,6 +47,13 @@ struct PrRankTag {
 template struct Reader<PrRankTag,
 	&ll_b_pagerank_pull_ext<ll_mlcsr_ro_graph, double>::G_pg_rank>;
 
+struct PrPushRankTag {
+	typedef double* ll_b_pagerank_push_ext<ll_mlcsr_ro_graph, double>::*type;
+	friend type get(PrPushRankTag);
+};
+template struct Reader<PrPushRankTag,
+	&ll_b_pagerank_push_ext<ll_mlcsr_ro_graph, double>::G_pg_rank>;
+
 struct SsspDistTag {
 	typedef float* ll_b_sssp_weighted<ll_mlcsr_ro_graph, float>::*type;
 	friend type get(SsspDistTag);
@@ -273,6 +280,21 @@ double llref_pagerank(void* gp, int level, int iters, double d, double* out) {
 	b.run();
 	double t = now_s() - t0;
 	if (out) memcpy(out, b.*get(PrRankTag()), sizeof(double) * g->V);
+	b.finalize();
+	return t;
+}
+
+// "pagerank_double_push" (ll_b_pagerank_push_double, pagerank.h:423-433):
+// returns run() seconds.
+double llref_pagerank_push(void* gp, int level, int iters, double d, double* out) {
+	RefGraph* g = (RefGraph*)gp;
+	View view(g, level);
+	ll_b_pagerank_push_double<ll_mlcsr_ro_graph> b(iters, d);
+	b.initialize(view.g);
+	double t0 = now_s();
+	b.run();
+	double t = now_s() - t0;
+	if (out) memcpy(out, b.*get(PrPushRankTag()), sizeof(double) * g->V);
 	b.finalize();
 	return t;
 }

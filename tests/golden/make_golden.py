@@ -8,7 +8,8 @@ level through the reference's CSR API and runs its benchmark kernels.
 Each fixture stores the level inputs (new edges with uint32 weights, and
 deletions, per level) and what the reference produced from them: the vertex
 table and edge-table slots of every level; for every snapshot, its adjacency
-in iteration order, degrees, PageRank (pagerank_double), BFS levels
+in iteration order, degrees, PageRank (pagerank_double and
+pagerank_double_push), BFS levels
 (sssp_unweighted), weighted SSSP distances (sssp_weighted), Brandes BC from
 fixed sources (bc_random's kernel, FP32, one thread: with more threads the
 reference's down-edge marking races, ll_bfs_template.h:619-640), and triangle
@@ -133,6 +134,8 @@ def make(name, fn):
             out[f"adj{l}_{dr}_off"], out[f"adj{l}_{dr}_nbr"] = off, nb
         out[f"outdeg{l}"] = S.degrees(-1)
         out[f"pr{l}"], _ = S.pagerank_pull(-1, PR_ITERS, DAMPING)
+        # one thread: the reference's atomic adds then run in vertex order
+        out[f"prpush{l}"], _ = S.pagerank_push(-1, PR_ITERS, DAMPING)
         out[f"bfs{l}"] = np.stack([S.bfs(-1, r)[0] for r in roots])
         out[f"bfscount{l}"] = np.array([S.bfs_count(-1, r)[0] for r in roots])
         out[f"sssp{l}"] = np.stack([S.sssp(-1, r)[0] for r in roots])

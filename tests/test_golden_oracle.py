@@ -41,6 +41,18 @@ def test_pagerank_bit_exact(golden):
         assert np.array_equal(pr, golden[f"pr{l}"]), l
 
 
+def test_pagerank_push_bit_exact(golden):
+    """The push restatement adds in vertex order, as the reference's atomic
+    adds run on one thread (how the golden vectors were made), so the bits
+    match; the pull and push results agree within FP64 rounding."""
+    O = build(golden)
+    for l in range(len(golden["levels"])):
+        pr = O.pagerank_push(l, int(golden["pr_iters"]), float(golden["damping"]))
+        assert np.array_equal(pr, golden[f"prpush{l}"]), l
+        rel = np.max(np.abs(pr - golden[f"pr{l}"]) / np.abs(golden[f"pr{l}"]))
+        assert rel <= 1e-12, (l, rel)
+
+
 def test_bfs_levels_exact(golden):
     O = build(golden)
     for l in range(len(golden["levels"])):
