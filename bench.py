@@ -395,7 +395,11 @@ def run_lg(args):
                     "algorithmic_bytes_per_step": bfs_bytes,
                     "bytes_model": "sum over roots of 8*E_reach + 4*V (fragment term "
                                    "omitted: lower bound)",
-                    "ms_per_step": bfs_s * 1e3, "roots": len(roots)}
+                    "ms_per_step": bfs_s * 1e3, "roots": len(roots),
+                    "note": "effective bandwidth: with --bfs multi the roots share one "
+                            "bit-parallel traversal, so the per-root model charges bytes the "
+                            "kernels never read and frac can exceed 1; --bfs single gives "
+                            "the one-root kernels' figure"}
 
     # e2e: newest level re-ingested from host, snapshot reopened, results to host
     e2e = None
