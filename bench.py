@@ -454,8 +454,11 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
     lg_store_ingest_level is reported as host_level.  Then one more step with
     a synchronisation after each phase (no overlap) gives the breakdown."""
     import torch
-    pr_host = torch.empty(V, dtype=torch.float64).pin_memory()
-    lv_host = torch.empty((len(roots), V), dtype=torch.int32).pin_memory()
+    # two sets of host result buffers: a pipelined step writes the set its
+    # predecessor is not still receiving
+    pr_bufs = [torch.empty(V, dtype=torch.float64).pin_memory() for _ in range(2)]
+    lv_bufs = [torch.empty((len(roots), V), dtype=torch.int32).pin_memory() for _ in range(2)]
+    cur = [0]
     L = hg.num_levels - 1
     desc = hg.level_desc(L)
     src, dst, dsrc, ddst, w = hg.level_input(L)
@@ -472,6 +475,7 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
             st.ingest_level(desc)
 
     def bfs():
+        lv_host = lv_bufs[cur[0]]
         if args.bfs == "multi":
             _, rs = s2.bfs_multi(roots, out=lv_host)
             return sum(r.reach_edges for r in rs)
@@ -483,22 +487,27 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
 
     s2 = None
 
-    def analytics(phase=None, overlap=True):
+    def analytics(phase=None, overlap=True, pipeline=False):
         # overlap: the BFS levels (16 x 4 B per vertex) go to the host on the
-        # store's copy stream (LG_OUTPUT_ASYNC) while PageRank runs
+        # store's copy stream (LG_OUTPUT_ASYNC) while PageRank runs.
+        # pipeline: in addition the step does not wait for its copies; the
+        # ranks reach the host while the next step rebuilds its level
         nonlocal s2
+        pr_host = pr_bufs[cur[0]]
         s2 = st.snapshot()
         if phase:
             phase("snapshot_open")
         s2.flatten(1)
         if overlap:
-            st.set_output_mode("async")
+            if not pipeline:
+                st.set_output_mode("async")
             reach = bfs()
             if phase:
                 phase("bfs")
             s2.pagerank_pull(args.pr_iters, 0.85, out=pr_host)
-            st.sync()                        # every result of the step is on the host
-            st.set_output_mode("sync")
+            if not pipeline:
+                st.sync()                    # every result of the step is on the host
+                st.set_output_mode("sync")
             if phase:
                 phase("pagerank_and_copies_to_host")
         else:
@@ -509,9 +518,11 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
             if phase:
                 phase("bfs_to_host")
         s2.close()
+        if pipeline:
+            cur[0] ^= 1
         return reach
 
-    def measure(kind, overlap=True):
+    def measure(kind, overlap=True, pipeline=False):
         load(kind)
         analytics(overlap=overlap)
         st.sync()
@@ -520,11 +531,15 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         edges = 0
+        if pipeline:
+            st.set_output_mode("async")
         e0.record(stream)
         for _ in range(args.steps):
             load(kind)
-            edges += args.pr_iters * E + analytics(overlap=overlap)
-        st.sync()
+            edges += args.pr_iters * E + analytics(overlap=overlap, pipeline=pipeline)
+        st.sync()                            # the last step's results are on the host
+        if pipeline:
+            st.set_output_mode("sync")
         e1.record(stream)
         stream.synchronize()
         h1, d1 = st.transfer_bytes()
@@ -535,11 +550,17 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
                 "d2h_bytes_per_step": (d1 - d0) // args.steps,
                 "ms_per_step": ms_max / args.steps}
 
-    out = measure("device")
+    out = measure("device", pipeline=True)
     out["includes"] = ("newest level rebuilt on the device from its edge delta (pinned host "
                        "arrays) + snapshot open + in-CSR flatten + BFS + PageRank, results "
-                       "copied to pinned host memory (BFS levels on the store's copy stream "
-                       "while PageRank runs; all on the host at the end of every step)")
+                       "copied to pinned host memory on the store's copy stream (BFS levels "
+                       "while PageRank runs, the ranks while the next step rebuilds its "
+                       "level, into alternating host buffers); every copy of every step "
+                       "inside the timed region")
+    stepwise = measure("device")
+    stepwise["includes"] = ("as the main figure, every step waiting for its own results "
+                            "before the next one starts")
+    out["step_synchronous"] = stepwise
     host = measure("host")
     host["includes"] = "as above, the level built on the host and ingested"
     out["host_level"] = host
