@@ -12,10 +12,14 @@ out-degree > 0) + free the flat CSR.
 value    = traversed edges per second of the device-resident step:
            (20 * E_live + sum over roots of E_reach) / step time  [GTEPS]
 e2e      = the same step through the C ABI with host buffers: every step
-           re-ingests the newest level from host memory (pinned staging),
-           reopens the snapshot and copies ranks and BFS levels back to host
+           rebuilds the newest level on the device from its edge delta in
+           pinned host memory, reopens the snapshot and copies the ranks and
+           BFS levels back to pinned host memory (on the store's copy
+           stream, overlapped with the following work; all copies inside the
+           timed region)
 roofline = the PageRank iteration kernel (pr_flat_step), HBM-bound
-bfs_roofline = the BFS phase against the per-root byte model (lower bound)
+bfs_roofline = the BFS phase against the per-root byte model (effective
+           bandwidth; the multi-source roots share one traversal)
 --impl reference times the reference's own OpenMP kernels (oracle/_ref, built
 from the reference source) on the host cores for the same step.
 
