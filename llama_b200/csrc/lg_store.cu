@@ -476,22 +476,25 @@ __global__ void walk_fragments(VtTab tab, int L, int minL, uint64_t V, uint32_t*
 __global__ void live_counts(SnapCsr g, uint32_t* out);
 
 // Sets the bit of every slot deleted at or before L and counts them in *count.
-// Slots of levels below minL are outside the window and have no bitset.
+// Slots of levels below minL are outside the window and have no bitset.  A
+// grid-stride loop: each warp adds its count once at the end (one atomic per
+// warp of a one-pass grid on the same counter serialised in L2).
 __global__ void mark_deletions(const uint2* dels, uint64_t n, int L, int minL,
 		uint32_t* const* del_words, unsigned long long* count) {
-	uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	bool hit = false;
-	if (i < n) {
-		uint2 d = dels[i];
-		uint32_t lv = d.y >> LG_BITS_LEVEL;
-		uint32_t ml = d.y & ((1u << LG_BITS_LEVEL) - 1u);
+	unsigned long long c = 0;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+			i += (uint64_t)gridDim.x * blockDim.x) {
+		const uint2 d = dels[i];
+		const uint32_t lv = d.y >> LG_BITS_LEVEL;
+		const uint32_t ml = d.y & ((1u << LG_BITS_LEVEL) - 1u);
 		if ((int)lv <= L && (int)lv >= minL && (int)ml <= L) {
 			atomicOr(del_words[lv] + (d.x >> 5), 1u << (d.x & 31));
-			hit = true;
+			c++;
 		}
 	}
-	const unsigned m = __ballot_sync(0xffffffffu, hit);
-	if ((threadIdx.x & 31u) == 0 && m) atomicAdd(count, (unsigned long long)__popc(m));
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+	if ((threadIdx.x & 31u) == 0 && c) atomicAdd(count, c);
 }
 
 // lb[r] = first vertex e with pos[e] >= r * kBlockSlots (pos has V + 1
@@ -580,7 +583,11 @@ static lg_status open_dir(lg_snapshot* sn, DevCsr& csr, SnapDir& d) {
 		LG_TRY(words.reserve(sizeof(uint32_t*) * LG_MAX_LEVELS));
 		LG_CUDA(cudaMemcpyAsync(words.p, lt.del, sizeof(lt.del),
 				cudaMemcpyHostToDevice, st), "deletion table");
-		mark_deletions<<<grid_for(csr.n_dels_dev, B), B, 0, st>>>(
+		int sms = 148;
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+		const unsigned mark_blocks = std::min<unsigned>(grid_for(csr.n_dels_dev, B),
+				(unsigned)sms * 8u);
+		mark_deletions<<<mark_blocks, B, 0, st>>>(
 				csr.dels.as<uint2>(), csr.n_dels_dev, L, minL,
 				(uint32_t* const*)words.p, counters.as<unsigned long long>() + 1);
 		LG_CUDA(cudaGetLastError(), "mark_deletions");
