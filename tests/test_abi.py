@@ -46,3 +46,38 @@ def test_store_create_without_gpu_fails_loudly():
     with pytest.raises(lb.LgError) as e:
         lb.Store()
     assert e.value.status == _lib.LG_ECUDA
+
+
+def test_plain_c_program_builds_and_links(tmp_path):
+    """A C99 host (what a cgo or other FFI stub compiles against) includes
+    both headers with warnings as errors, links liblg.so and calls it: the
+    version string, and a store that either opens (GPU present) or fails
+    with LG_ECUDA and a message (no GPU), never a CPU fallback."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "host.c"
+    src.write_text(
+        '#include "lg.h"\n#include "lg_host.h"\n#include <stdio.h>\n'
+        "int main(void) {\n"
+        "  lg_store* s = NULL;\n"
+        "  lg_store_opts o = {0};\n"
+        "  lg_status st = lg_store_create(&s, &o);\n"
+        "  printf(\"%s %d\\n\", lg_version(), (int)st);\n"
+        "  if (st == LG_OK) return lg_store_destroy(s) == LG_OK ? 0 : 1;\n"
+        "  char msg[256];\n"
+        "  lg_last_error(msg, sizeof msg);\n"
+        "  return (st == LG_ECUDA && msg[0] != 0) ? 0 : 2;\n"
+        "}\n")
+    exe = tmp_path / "host"
+    libdir = os.path.dirname(lb.LIB_PATH)
+    subprocess.check_call([gcc, "-std=c99", "-Wall", "-Wextra", "-Werror",
+                           "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                           "-L", libdir, "-llg", "-Wl,-rpath," + libdir])
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.stdout, r.stderr)
+    version, status = r.stdout.split()
+    assert version == lb.lib.lg_version().decode()
+    assert int(status) in (_lib.LG_OK, _lib.LG_ECUDA)
