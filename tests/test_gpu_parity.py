@@ -334,7 +334,8 @@ def _write_level_files(golden, tmp_path):
     return files
 
 
-@pytest.mark.parametrize("task", ["pagerank_double", "bfs_count", "sssp_weighted", "tc_u"])
+@pytest.mark.parametrize("task", ["pagerank_double", "pagerank_double_push", "bfs_count",
+                                  "sssp_weighted", "tc_u"])
 def test_cli_return_value_matches_reference(golden, tmp_path, task):
     """`lg_benchmark -r TASK FILE...` prints the reference task's return value."""
     import os
@@ -352,10 +353,11 @@ def test_cli_return_value_matches_reference(golden, tmp_path, task):
     out = subprocess.run([exe, "-r", task, "-R", str(root), "-n", str(int(golden["pr_iters"]))]
                          + files, capture_output=True, text=True, check=True).stdout
     ret = float(out.strip().splitlines()[-1].split(":")[1])
-    if task == "pagerank_double":
+    if task in ("pagerank_double", "pagerank_double_push"):
         if used != V:
             pytest.skip("largest vertex id is isolated")
-        assert abs(ret - float(np.sum(golden[f"pr{L}"]))) <= 1e-9
+        key = "pr" if task == "pagerank_double" else "prpush"
+        assert abs(ret - float(np.sum(golden[f"{key}{L}"]))) <= 1e-9
     elif task == "bfs_count":
         assert ret == golden[f"bfscount{L}"][0]
     elif task == "sssp_weighted":
