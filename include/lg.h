@@ -316,7 +316,10 @@ lg_status lg_snapshot_is_flat(const lg_snapshot* snap, int dir, int* flat);
  * ll_b_pagerank_pull_ext<Graph,double>::run (benchmark/benchmarks/pagerank.h:98-182).
  * pr0 = 1/N with N = max_nodes; each of `iterations` steps sets
  * pr'[t] = (1-d)/N + d * sum_{w in in(t)} pr[w] / out_degree(w); dangling mass
- * is dropped.  ranks: double[max_nodes].  Requires the in-CSR. */
+ * is dropped.  ranks: double[max_nodes].  Requires the in-CSR.
+ * iterations = 0 returns pr0; the reference's do-while loop
+ * (pagerank.h:133-178) runs one iteration when max is 0, so a caller that
+ * forwards the reference's -n value passes max(n, 1). */
 lg_status lg_pagerank_pull(lg_snapshot* snap, int iterations, double damping,
 		double* ranks);
 

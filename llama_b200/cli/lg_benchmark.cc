@@ -198,14 +198,17 @@ int main(int argc, char** argv) {
 		double ts = now_ms();
 		if (task == "pagerank_double" || task == "pagerank") {
 			std::vector<double> pr(V);
-			CHECK(lg_pagerank_pull(snap, iters, 0.85, pr.data()), "lg_pagerank_pull");
+			// the reference's do-while loop runs one iteration for -n 0
+			CHECK(lg_pagerank_pull(snap, std::max(iters, 1), 0.85, pr.data()),
+					"lg_pagerank_pull");
 			double s = 0;
 			for (double x : pr) s += x;
 			ret = s;
 			if (of && run == count - 1) print_part(of, pr.data(), V, "%0.6lf");
 		} else if (task == "pagerank_double_push") {
 			std::vector<double> pr(V);
-			CHECK(lg_pagerank_push(snap, iters, 0.85, pr.data()), "lg_pagerank_push");
+			CHECK(lg_pagerank_push(snap, std::max(iters, 1), 0.85, pr.data()),
+					"lg_pagerank_push");
 			double s = 0;
 			for (double x : pr) s += x;
 			ret = s;
