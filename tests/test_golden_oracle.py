@@ -141,3 +141,17 @@ def test_oracle_window_matches_filtered_reference_iteration(golden):
                 assert np.array_equal(wo, eo) and np.array_equal(wn, en), (l, m, dr)
                 if dr == 0:
                     assert np.array_equal(O.degrees(l, 0), ecnt.astype(np.uint32))
+
+
+def test_oracle_push_equals_pull_on_windows(golden):
+    """On sliding windows too, the push restatement gives the pull vector
+    within FP64 rounding (the same sums, added in another order)."""
+    iters, d = int(golden["pr_iters"]), float(golden["damping"])
+    for l in range(1, len(golden["levels"])):
+        for m in range(1, l + 1):
+            O = build(golden)
+            O.set_min_level(m)
+            pull = O.pagerank_pull(l, iters, d)
+            push = O.pagerank_push(l, iters, d)
+            rel = np.max(np.abs(push - pull) / np.abs(pull))
+            assert rel <= 1e-12, (l, m, rel)
