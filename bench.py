@@ -59,7 +59,8 @@ def parse():
     p.add_argument("--no-extras", action="store_true",
                    help="skip the secondary kernels (SSSP, TC, SCC, BC, PPR, adjoint)")
     p.add_argument("--kron-scale", type=int, default=21)
-    p.add_argument("--bc-sources", type=int, default=256)
+    p.add_argument("--bc-sources", type=int, default=4096,
+                   help="sources of the batched BC run (64 per pass)")
     p.add_argument("--adjoint-scale", type=int, default=20)
     p.add_argument("--out", default=None, help="also write the JSON line here")
     return p.parse_args()
