@@ -1,13 +1,13 @@
 #!/usr/bin/env python
 """Benchmark: PageRank pull + BFS GTEPS over a multiversion R-MAT store.
 
-Workload (default): directed R-MAT scale 24 (2^24 vertices, 16 * 2^24 draws,
-a/b/c/d = .57/.19/.19/.05, self-loops and duplicates removed, seed 2), split
-into 8 levels: a seeded 90 % of the edges form level 0, levels 1..7 each add
-~1.4 % and delete 0.2 % of the live edges (deletion marks in older levels).
-One step on the latest snapshot = flatten its in-CSR (lg_snapshot_flatten)
-+ FP64 PageRank pull, 20 iterations, d = 0.85 + BFS from 16 roots (seed 3,
-out-degree > 0) + free the flat CSR.
+Workload (default, --workload c2): directed R-MAT scale 24 (2^24 vertices,
+16 * 2^24 draws, a/b/c/d = .57/.19/.19/.05, self-loops and duplicates
+removed, seed 2), split into 8 levels: a seeded 90 % of the edges form level
+0, levels 1..7 each add ~1.4 % and delete 0.2 % of the live edges (deletion
+marks in older levels).  One step on the latest snapshot = flatten its
+in-CSR (lg_snapshot_flatten) + FP64 PageRank pull, 20 iterations, d = 0.85
++ BFS from 16 roots (seed 3, out-degree > 0) + free the flat CSR.
 
 value    = traversed edges per second of the device-resident step:
            (20 * E_live + sum over roots of E_reach) / step time  [GTEPS]
@@ -17,11 +17,19 @@ e2e      = the same step through the C ABI with host buffers: every step
            BFS levels back to pinned host memory (on the store's copy
            stream, overlapped with the following work; all copies inside the
            timed region)
-roofline = the PageRank iteration kernel (pr_flat_step), HBM-bound
-bfs_roofline = the BFS phase against the per-root byte model (effective
-           bandwidth; the multi-source roots share one traversal)
+roofline = the PageRank iteration kernel (pr_flat_step), HBM-bound; the
+           secondary kernels' figures are under extras
+parity   = the step's outputs against the reference's own kernels on the
+           same store (PageRank <= 1e-12, BFS levels exact), the triangle
+           count against the oracle, and the secondary workloads' checks
+           (batched BC, PPR, adjoint gradients by finite differences)
 --impl reference times the reference's own OpenMP kernels (oracle/_ref, built
-from the reference source) on the host cores for the same step.
+from the reference source) on the host cores for the same workload; that
+process builds its inputs with the oracle's generator and never loads the
+engine.
+--workload c5 runs the large full suite instead (R-MAT scale 26, uint32
+weights, 4 levels with 1 % deletions; PageRank, BFS, delta-stepping SSSP,
+SCC, batched BC), each kernel beside the reference's timing.
 
 N > 1 (torchrun): independent replicas, one store per GPU (the path does not
 shard), weak scaling; value = all ranks' edges / max-over-ranks time.
@@ -62,24 +70,85 @@ def parse():
     p.add_argument("--bc-sources", type=int, default=4096,
                    help="sources of the batched BC run (64 per pass)")
     p.add_argument("--adjoint-scale", type=int, default=20)
+    p.add_argument("--fd-probes", type=int, default=64,
+                   help="edges and vertices probed by finite differences (each)")
+    p.add_argument("--workload", default="c2", choices=["c2", "c5"])
+    p.add_argument("--no-parity", action="store_true",
+                   help="skip the checks of the outputs against the reference / oracle")
+    p.add_argument("--traffic", type=float, default=None,
+                   help="DRAM bytes per pr_flat_step launch measured by ncu for this "
+                        "workload, reported as roofline.traffic")
     p.add_argument("--out", default=None, help="also write the JSON line here")
     return p.parse_args()
 
 
+def rmat_params(scale, seed, levels, level0, delete, weight_max=0):
+    """Generator fields (lg_graph_spec) of a multiversion R-MAT workload, as
+    llama_b200.workloads.rmat_multiversion sets them (plain values, so the
+    reference arm needs no engine import)."""
+    return dict(kind=0, scale=scale, edge_factor=16.0, a=0.57, b=0.19, c=0.19, seed=seed,
+                symmetrize=False, num_levels=levels, level0_fraction=level0,
+                delete_fraction=delete, split_seed=seed * 1000 + 17,
+                weight_max=weight_max, weight_seed=seed * 1000 + 29)
+
+
+def kron_params(scale, seed, levels):
+    """Generator fields of the symmetric Kronecker workload, as
+    llama_b200.workloads.kronecker_symmetric sets them."""
+    return dict(kind=1, scale=scale, edge_factor=16.0, a=0.57, b=0.19, c=0.19, seed=seed,
+                symmetrize=True, num_levels=levels, level0_fraction=1.0 / levels,
+                delete_fraction=0.0, split_seed=seed * 1000 + 17, weight_max=0,
+                weight_seed=0)
+
+
 def workload(args):
-    from llama_b200 import workloads
-    spec = workloads.rmat_multiversion(scale=args.scale, seed=2, levels=args.levels,
-                                       level0=0.90, delete=0.002, weight_max=255)
-    cfg = {"workload": f"rmat{args.scale}_{args.levels}level_del0.2pct",
-           "graph": f"directed R-MAT scale {args.scale}, edge factor 16, "
-                    f"{args.levels} levels (90% in level 0, 0.2% deletions per level)",
-           "step": f"flatten the in-CSR + PageRank pull FP64 x{args.pr_iters} iterations "
-                   f"+ BFS from {args.roots} roots, latest snapshot",
-           "bfs_mode": ("all roots in one multi-source call (lg_bfs_multi, 64 roots per "
-                        "bit-parallel pass; each row equals a single-root BFS)"
-                        if args.bfs == "multi" else "one lg_bfs call per root"),
-           "pr_iterations": args.pr_iters, "damping": 0.85, "bfs_roots": args.roots}
-    return spec, cfg
+    """(generator fields, config) of the bench workload; the config is the
+    same in both arms."""
+    if args.workload == "c5":
+        params = rmat_params(args.scale, 7, args.levels, 0.85, 0.01, weight_max=255)
+        cfg = {"workload": f"rmat{args.scale}_{args.levels}level_del1pct_weighted",
+               "graph": f"directed R-MAT scale {args.scale}, edge factor 16, uint32 weights "
+                        f"U[1,255], {args.levels} levels (85% in level 0, the rest split "
+                        "evenly, 1% of the live edges deleted at each later level)",
+               "step": "PageRank pull FP64 x20, BFS from 64 roots, delta-stepping SSSP "
+                       "(delta 32) from 8 roots, SCC, batched BC over 1024 sources, latest "
+                       "snapshot",
+               "pr_iterations": args.pr_iters, "damping": 0.85}
+    else:
+        params = rmat_params(args.scale, 2, args.levels, 0.90, 0.002, weight_max=255)
+        cfg = {"workload": f"rmat{args.scale}_{args.levels}level_del0.2pct",
+               "graph": f"directed R-MAT scale {args.scale}, edge factor 16, "
+                        f"{args.levels} levels (90% in level 0, 0.2% deletions per level)",
+               "step": f"flatten the in-CSR + PageRank pull FP64 x{args.pr_iters} iterations "
+                       f"+ BFS from {args.roots} roots, latest snapshot",
+               "bfs_mode": ("all roots in one multi-source call (lg_bfs_multi, 64 roots per "
+                            "bit-parallel pass; each row equals a single-root BFS)"
+                            if args.bfs == "multi" else "one lg_bfs call per root"),
+               "pr_iterations": args.pr_iters, "damping": 0.85, "bfs_roots": args.roots}
+    cfg["parallelism"] = f"replicas{args.gpus}"
+    cfg["l2"] = ("inputs larger than L2 (126 MB): the store's level arrays take several GB "
+                 "on the device")
+    return params, cfg
+
+
+def max_rel(a, b):
+    """max |a - b| / |b| over the entries (0 where both are 0)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    d = np.abs(a - b)
+    den = np.maximum(np.abs(b), np.abs(a))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.where(d == 0, 0.0, d / np.where(den == 0, 1.0, den))
+    return float(r.max()) if r.size else 0.0
+
+
+def engine_loaded():
+    """True if this process has mapped the engine library (liblg.so)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return any("liblg.so" in line for line in f)
+    except OSError:
+        return None
 
 
 def dist_init(args):
@@ -184,39 +253,30 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per pr_flat_step launch at this workload, from the line
-    `traffic_bytes_per_launch: N` of the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "pr_flat_step_rmat24.md")
-    try:
-        with open(path) as f:
-            for line in f:
-                if line.startswith("traffic_bytes_per_launch:"):
-                    return {"dram_bytes_per_launch_scaled": float(line.split(":")[1])}
-    except (OSError, ValueError):
-        pass
-    return None
-
-
 def run_reference(args):
+    """The reference's OpenMP kernels (oracle/_ref) on this host's cores, on
+    the same workload, config and metric as the device arm.  The inputs come
+    from the oracle's generator, so this process never loads the engine."""
     ws, rank, local = dist_init(args)
     if rank != 0:
         return
-    from llama_b200 import HostGraph
-    from oracle.bind import Reference, ref_available
-    spec, cfg = workload(args)
+    from oracle.bind import Reference, generate_levels, pick_roots, ref_available
+    params, cfg = workload(args)
     if not ref_available():
         print(json.dumps({"impl": "reference",
                           "unavailable": "oracle/_ref/libllref.so was not built"}))
         return
-    hg = HostGraph.from_spec(spec)
-    R = Reference(spec.max_nodes)
-    for l in range(hg.num_levels):
-        R.add_level(*hg.level_input(l)[:4])
-    del hg
-    from llama_b200 import workloads
+    t0 = time.time()
+    levels = generate_levels(**params)
+    V = 1 << params["scale"]
+    R = Reference(V)
+    for lv in levels:
+        R.add_level(*lv[:4])
+    del levels
+    build_s = time.time() - t0
     deg = R.degrees(-1)
-    roots = workloads.pick_roots(deg, args.roots, seed=3)
+    n_roots = 64 if args.workload == "c5" else args.roots
+    roots = pick_roots(deg, n_roots, seed=3)
     E = int(deg.sum())
     cores = Reference.max_threads()
 
@@ -247,16 +307,23 @@ def run_reference(args):
     line = {"metric": METRIC, "value": gteps, "unit": "GTEPS", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * tot_t / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded R-MAT generator, no dataset)",
             "config": cfg,
             "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": cores,
                              "kind": "reference",
-                             "sample": f"each step = a quarter of the device step: "
-                                       f"pagerank_double x{q_it} + sssp_unweighted BFS "
-                                       f"from {q_roots} of the {len(roots)} roots in turn, "
-                                       "on the same store, run() time only"},
+                             "sample": f"each step = a quarter of the device step in the same "
+                                       f"proportions: pagerank_double x{q_it} + "
+                                       f"sssp_unweighted BFS from {q_roots} of the "
+                                       f"{len(roots)} roots in turn, on the same store, run() "
+                                       "time only (the rate is comparable, the work per step "
+                                       "is a quarter)"},
             "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "store_build_s": build_s,
+            "engine_loaded": engine_loaded(),
+            "inputs": "levels from the oracle's generator (oracle/lgo.cpp lgo_gen_create), "
+                      "the same edges as the device arm's"}
     emit(line, args)
 
 
@@ -273,8 +340,9 @@ def run_lg(args):
     ws, rank, local = dist_init(args)
     torch.cuda.set_device(local)
     from llama_b200 import HostGraph, Store, workloads
-    spec, cfg = workload(args)
-    cfg["parallelism"] = f"replicas{ws}"
+    from llama_b200.graph import GraphSpec
+    params, cfg = workload(args)
+    spec = GraphSpec(**params)
     t0 = time.time()
     hg = HostGraph.from_spec(spec)
     build_s = time.time() - t0
@@ -342,6 +410,9 @@ def run_lg(args):
     ms = t_start.elapsed_time(t_end)
     ms_max, edges_all = reduce_max_sum(ws, ms, edges)
     value = edges_all / (ms_max / 1e3) / 1e9
+    # the last timed step's outputs, checked against the reference below
+    step_pr = pr_dev.cpu().numpy()
+    step_lv = lv_dev.cpu().numpy()
 
     # roofline of the PageRank iteration kernel (pr_flat_step + its fix-up
     # over the flat live in-edges): one iteration = the difference between a
@@ -364,8 +435,6 @@ def run_lg(args):
     launch_s = statistics.median(diffs) / 1e3
     peak, peak_kind = measured_peak()
     achieved = pr_bytes / launch_s / 1e9
-    # the committed ncu figure is for the default workload only
-    traffic = profiled_traffic() if (args.scale, args.levels) == (24, 8) else None
     roofline = {"bound": "hbm", "kernel": "pr_flat_step", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
@@ -380,10 +449,10 @@ def run_lg(args):
                 "launch_ms_source": "CUDA events on the store's stream: "
                                     "(t(2k iterations) - t(k iterations)) / k, median of 3",
                 "pr_call_ms": pr_ms / args.steps,
-                "traffic": traffic["dram_bytes_per_launch_scaled"] if traffic else None,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one "
-                                  "full-size launch (profiles/pr_flat_step_rmat24.md)"
-                                  if traffic else None}
+                "traffic": args.traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                  "full-size launch, passed with --traffic"
+                                  if args.traffic else "not measured in this run"}
 
     # BFS of the step, against the per-root byte model of the path's survey:
     # sum over roots of (4 B id + 4 B neighbour level per reached out-edge)
@@ -406,20 +475,29 @@ def run_lg(args):
                             "kernels never read and frac can exceed 1; --bfs single gives "
                             "the one-root kernels' figure"}
 
+    parity = {}
     # e2e: newest level re-ingested from host, snapshot reopened, results to host
     e2e = None
     if not args.no_e2e:
         sn.close()
         sn = None
-        e2e = run_e2e(args, ws, st, hg, V, E, roots, stream)
+        e2e, host_pr, host_lv = run_e2e(args, ws, st, hg, V, E, roots, stream)
+        # the e2e step rebuilds its newest level on the device: its results
+        # must be the device-resident step's, bit for bit
+        parity["e2e_outputs_equal_step"] = bool(np.array_equal(host_pr, step_pr)
+                                                and np.array_equal(host_lv, step_lv))
+        del host_pr, host_lv
 
     ext = None
     if not args.no_extras:
-        ext = extras(args, st, stream, local)
+        ext = extras(args, st, stream, local, parity)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(hg, spec, roots, args)
+        cpu = cpu_baseline(hg, spec, roots, args, step_pr, step_lv, ext, parity)
+    del step_pr, step_lv
+    checks = [v for k, v in parity.items() if k.endswith("_ok") or k.endswith("_equal_step")]
+    parity["all_ok"] = bool(checks) and all(checks)
 
     line = {"metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": ws,
             "steps": args.steps, "warmup": max(3, args.warmup),
@@ -437,9 +515,10 @@ def run_lg(args):
                                 / (bfs_ms / 1e3) / 1e9, "last_reach_edges": reach}},
             "graph": {"max_nodes": V, "live_edges": E, "in_slots": ins["slots"],
                       "in_fragments": ins["fragments"], "levels": hg.num_levels,
-                      "host_build_s": build_s, "ingest_s": ingest_s},
+                      "host_build_s": build_s, "ingest_s": ingest_s,
+                      "device_bytes": st.device_bytes},
             "roofline": roofline, "bfs_roofline": bfs_roofline, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "cpu_baseline": cpu, "extras": ext}
+            "clocks": clk, "cpu_baseline": cpu, "parity": parity, "extras": ext}
     if rank == 0:
         emit(line, args)
     if sn is not None:
@@ -588,7 +667,8 @@ def run_e2e(args, ws, st, hg, V, E, roots, stream):
     phase("build_level")
     analytics(phase, overlap=False)
     out["phases_ms"] = phases
-    return out
+    # the host buffers this last (synchronised) step wrote
+    return out, pr_bufs[cur[0]].numpy(), lv_bufs[cur[0]].numpy()
 
 
 def _timed(stream, fn):
@@ -602,17 +682,27 @@ def _timed(stream, fn):
     return r, e0.elapsed_time(e1)
 
 
-def extras(args, st, stream, device):
-    """Secondary kernels, each timed once with CUDA events on the store's
-    stream after a warm-up call: SSSP / triangle counting / SCC on the main
-    store; batched vs plain BC and the PPR block on a symmetric Kronecker
-    store; adjoint vs forward PageRank on a weighted R-MAT."""
+def extras(args, st, stream, device, parity):
+    """Secondary kernels, each timed with CUDA events on the store's stream
+    after a warm-up call, each with its byte model (the survey of the path,
+    section 8(d)) against the measured HBM peak: SSSP / triangle counting /
+    SCC / one-root BFS on the main store; batched vs plain BC and the PPR
+    block on a symmetric Kronecker store; adjoint vs forward PageRank on a
+    weighted R-MAT.  Output checks go into `parity`."""
     import torch
-    import numpy as np
     from llama_b200 import HostGraph, Store, workloads
     from llama_b200.graph import ppr
     out = {}
     dev = f"cuda:{device}"
+    peak, _ = measured_peak()
+
+    def roof(bytes_, ms, model, note=None):
+        gbs = bytes_ / (ms / 1e3) / 1e9
+        r = {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+             "frac": gbs / peak, "algorithmic_bytes": bytes_, "bytes_model": model}
+        if note:
+            r["note"] = note
+        return r
 
     def guard(name, fn):
         try:
@@ -625,6 +715,22 @@ def extras(args, st, stream, device):
         try:
             V, E = sn.max_nodes, sn.num_edges
             res = {}
+            # one-root direction-optimising BFS, the 16 bench roots one call each
+            broots = workloads.pick_roots(sn.out_degrees(), args.roots, seed=3)
+            lv1 = torch.empty(V, dtype=torch.int32, device=dev)
+            sn.bfs(int(broots[0]), out=lv1)
+            ms, reach = 0.0, 0
+            for r in broots:
+                (_, rr), t = _timed(stream, lambda: sn.bfs(int(r), out=lv1))
+                ms += t
+                reach += rr.reach_edges
+            res["bfs_single_root"] = {
+                "roots": len(broots), "ms": ms, "gteps": reach / (ms / 1e3) / 1e9,
+                "roofline": roof(8 * reach + 4 * V * len(broots), ms,
+                                 "sum over roots of 4 B id + 4 B neighbour level per reached "
+                                 "out-edge + 4 B level per vertex",
+                                 "lower bound of the per-root model (the 12 B per reached "
+                                 "fragment term is left out)")}
             roots = workloads.pick_roots(sn.out_degrees(), 8, seed=13)
             dist = torch.empty(V, dtype=torch.int32, device=dev)
             sn.sssp(int(roots[0]), 32, out=dist)
@@ -636,9 +742,13 @@ def extras(args, st, stream, device):
                 rounds += rr.rounds
                 buckets += rr.buckets
                 relax += rr.relaxations
-            res["sssp_delta32_8roots"] = {"ms": ms, "gteps": reach / (ms / 1e3) / 1e9,
-                                          "rounds": rounds, "buckets": buckets,
-                                          "relaxations_per_reached_edge": relax / max(reach, 1)}
+            res["sssp_delta32_8roots"] = {
+                "ms": ms, "gteps": reach / (ms / 1e3) / 1e9, "rounds": rounds,
+                "buckets": buckets, "relaxations_per_reached_edge": relax / max(reach, 1),
+                "roofline": roof(12 * reach + 4 * V * buckets, ms,
+                                 "sum over roots of 12 B (id, weight, distance) per reached "
+                                 "edge + 4 B per vertex per bucket",
+                                 "lower bound: every reached edge relaxed once")}
             # the same roots on the snapshot with its out-CSR flattened once
             _, fms = _timed(stream, lambda: sn.flatten(0))
             reach, ms = 0, 0.0
@@ -665,7 +775,11 @@ def extras(args, st, stream, device):
             lab = torch.empty(V, dtype=torch.int64, device=dev)
             sn.scc(out=lab)
             (_, sr), ms = _timed(stream, lambda: sn.scc(out=lab))
-            res["scc"] = {"ms": ms, "components": sr.components, "gteps": E / (ms / 1e3) / 1e9}
+            res["scc"] = {"ms": ms, "components": sr.components, "gteps": E / (ms / 1e3) / 1e9,
+                          "steps": sr.steps, "rounds": sr.rounds,
+                          "roofline": roof(sr.steps * (4 * E + 8 * V), ms,
+                                           "traversal steps x (4 B per live edge + 8 B per "
+                                           "vertex)")}
             return res
         finally:
             sn.close()
@@ -688,23 +802,41 @@ def extras(args, st, stream, device):
                 s64 = src[:64]
                 t64 = statistics.median(
                     _timed(stream, lambda: sn.bc(s64, batched=True, out=bc))[1] for _ in range(3))
+                bc_batched = bc.cpu().numpy()
                 sn.bc(s64[:2], batched=False, out=bc)
                 tp = statistics.median(
                     _timed(stream, lambda: sn.bc(s64, batched=False, out=bc))[1] for _ in range(3))
+                bc_plain = bc.cpu().numpy()
+                passes = (len(src) + 63) // 64
                 res = {"bc": {"graph": f"Kronecker scale {args.kron_scale}, symmetric, 4 levels",
                               "batched_ms_per_source": tb / len(src),
                               "batched_gteps": 2 * E * len(src) / (tb / 1e3) / 1e9,
                               "sources_batched": len(src),
                               "same_64_sources": {"batched_ms": t64, "plain_ms": tp,
                                                   "batched_speedup": tp / t64},
-                              "timing": "median of 3 runs each"}}
+                              "timing": "median of 3 runs each",
+                              "roofline": roof(passes * (2 * 12 * E + V * 64 * 16 * 2), tb,
+                                               "per 64-source pass: 2 sweeps x 12 B per "
+                                               "scanned edge + 2 x 16 B per vertex per source",
+                                               "lower bound: every live edge scanned once "
+                                               "per sweep")}}
                 seeds = workloads.pick_roots(sn.out_degrees(), 256, seed=15)
                 out_ppr = torch.empty((4, V, 256), dtype=torch.float64, device=dev)
                 ppr(snaps, seeds[:32], iterations=2, out=out_ppr[:, :, :32].contiguous())
                 _, tq = _timed(stream, lambda: ppr(snaps, seeds, iterations=20, out=out_ppr))
                 e_all = sum(s.num_edges for s in snaps)
-                res["ppr"] = {"K": 256, "iterations": 20, "snapshots": 4, "ms": tq,
-                              "gteps": 20 * e_all * 256 / (tq / 1e3) / 1e9}
+                K = 256
+                res["ppr"] = {"K": K, "iterations": 20, "snapshots": 4, "ms": tq,
+                              "gteps": 20 * e_all * K / (tq / 1e3) / 1e9,
+                              "roofline": roof(20 * (e_all * (4 + 8 * K) + 4 * 2 * 8 * K * V), tq,
+                                               "per iteration and snapshot: E_live x (4 + 8K) "
+                                               "+ 2 x 8 B x K x V")}
+                if not args.no_parity:
+                    cols = [0, K - 1]
+                    ppr_cols = out_ppr[:, :, cols].cpu().numpy()
+                    del out_ppr
+                    res["parity"] = kron_parity(hg, V, s64, bc_batched, bc_plain, seeds[cols],
+                                                ppr_cols, parity)
                 return res
             finally:
                 for s in snaps:
@@ -716,7 +848,7 @@ def extras(args, st, stream, device):
         with Store(device=device, stream=stream.cuda_stream) as s3:
             s3.ingest(hg)
             with s3.snapshot() as sn:
-                V = sn.max_nodes
+                V, E = sn.max_nodes, sn.num_edges
                 off, nb = sn.adjacency(0)
                 rng = np.random.default_rng(4)
                 raw = rng.uniform(0.5, 1.5, len(nb))
@@ -737,11 +869,24 @@ def extras(args, st, stream, device):
                 dv = torch.empty(V, dtype=torch.float64, device=dev)
                 (_, _, br), tb = _timed(stream, lambda: tape.backward(g, dw, dv))
                 tape.close()
-                return {"graph": f"R-MAT scale {args.adjoint_scale}, FP64 weights U[0.5,1.5] "
-                                 "row-normalised, Dirichlet(1) teleport, tol 1e-12",
-                        "forward_ms": tf, "forward_iterations": fr.iterations,
-                        "backward_ms": tb, "backward_iterations": br.iterations,
-                        "backward_over_forward": tb / tf}
+                it_bytes = E * (4 + 8 + 8)
+                res = {"graph": f"R-MAT scale {args.adjoint_scale}, FP64 weights U[0.5,1.5] "
+                                "row-normalised, Dirichlet(1) teleport, tol 1e-12",
+                       "forward_ms": tf, "forward_iterations": fr.iterations,
+                       "backward_ms": tb, "backward_iterations": br.iterations,
+                       "backward_over_forward": tb / tf,
+                       "forward_ms_per_iteration": tf / max(fr.iterations, 1),
+                       "roofline_forward": roof(it_bytes * fr.iterations, tf,
+                                                "per iteration E_live x (4 B id + 8 B weight "
+                                                "+ 8 B gathered score)",
+                                                "the call: weight gather into in-edge order + "
+                                                "the iterations + result copy"),
+                       "roofline_backward": roof(it_bytes * br.iterations, tb,
+                                                 "per iteration E_live x (4 + 8 + 8) B")}
+                if not args.no_parity:
+                    res["fd_check"] = adjoint_fd(sn, w, v, x, u, T, dw, dv, srcv, nb,
+                                                 args.fd_probes, dev, parity)
+                return res
 
     guard("kronecker", on_kron)
     guard("main_store", on_main)
@@ -749,9 +894,129 @@ def extras(args, st, stream, device):
     return out
 
 
-def cpu_baseline(hg, spec, roots, args):
-    """Reference OpenMP kernels on this host's cores, one step (bounded)."""
-    from oracle.bind import Reference, ref_available
+def kron_parity(hg, V, s64, bc_batched, bc_plain, seeds, ppr_cols, parity):
+    """C4 outputs at size: batched and plain BC on the same 64 sources against
+    each other and against the oracle's FP64 Brandes (lgo_csr_bc); two PPR
+    columns (the first and the last of the K block) on every snapshot against
+    the oracle's PPR (lgo_csr_ppr).  The oracle runs on CSRs built from the
+    level inputs with numpy (the workload has no deletions, so snapshot l
+    holds the edges of levels 0..l)."""
+    from oracle.bind import csr_bc, csr_from_edges, csr_ppr
+    t0 = time.time()
+    srcs, dsts, lvl = [], [], []
+    for l in range(hg.num_levels):
+        a, b = hg.level_input(l)[:2]
+        srcs.append(a)
+        dsts.append(b)
+        lvl.append(np.full(len(a), l, np.uint8))
+    src = np.concatenate(srcs)
+    dst = np.concatenate(dsts)
+    lvl = np.concatenate(lvl)
+    del srcs, dsts
+    off, nb = csr_from_edges(V, src, dst)
+    obc = csr_bc(V, off, nb, s64)
+    del off, nb
+    r = {"bc_sources": len(s64),
+         "bc_batched_vs_oracle_max_rel": max_rel(bc_batched, obc),
+         "bc_plain_vs_oracle_max_rel": max_rel(bc_plain, obc),
+         "bc_batched_vs_plain_max_rel": max_rel(bc_batched, bc_plain)}
+    r["bc_ok"] = max(r["bc_batched_vs_oracle_max_rel"], r["bc_plain_vs_oracle_max_rel"]) <= 1e-9
+    worst = 0.0
+    for l in range(hg.num_levels):
+        m = lvl <= l
+        s_l, d_l = src[m], dst[m]
+        ioff, inb = csr_from_edges(V, d_l, s_l)
+        od = np.bincount(s_l, minlength=V).astype(np.uint32)
+        want = csr_ppr(V, ioff, inb, od, seeds, 20, 0.85)
+        worst = max(worst, max_rel(ppr_cols[l], want))
+    r["ppr_columns_checked"] = f"{len(seeds)} of 256 (the first and the last) on each of " \
+                               f"{hg.num_levels} snapshots"
+    r["ppr_max_rel"] = worst
+    r["ppr_ok"] = worst <= 1e-12
+    r["oracle_s"] = time.time() - t0
+    parity["kron_bc_ok"] = r["bc_ok"]
+    parity["kron_bc_max_rel"] = max(r["bc_batched_vs_oracle_max_rel"],
+                                    r["bc_plain_vs_oracle_max_rel"])
+    parity["kron_ppr_ok"] = r["ppr_ok"]
+    parity["kron_ppr_max_rel"] = worst
+    return r
+
+
+def adjoint_fd(sn, w, v, x, u, T, dw, dv, srcv, nb, probes, dev, parity):
+    """Gradients of L = sum_T (x_t - 1.2 u_t)^2 against FP64 central
+    differences, h = 1e-6, on `probes` random edges and vertices.
+
+    (L(p + h) - L(p - h)) / 2h is formed from the perturbed fixed points'
+    differences from x rather than from the two perturbed scores: with
+    P' = P + h on edge a -> b, x' - x solves  D = d P'^T D + d h x[a] e_b,
+    which the forward computes exactly (teleport e_b, weights P', scaled),
+    and L' - L = sum_T D (2 (x - t) + D).  This is the same central
+    difference in exact arithmetic, without subtracting two nearly equal
+    scores (at 2^20 vertices the scores are ~1e-6 and the change ~1e-18, so
+    plain subtraction leaves only a few correct digits).  A teleport probe
+    is linear: D = +-h (1-d)(I - d P^T)^-1 e_t."""
+    import torch
+    d = 0.85
+    h = 1e-6
+    V = x.numel()
+    rng = np.random.default_rng(5)
+    pe = rng.choice(len(nb), probes, replace=False)
+    pv = rng.choice(V, probes, replace=False)
+    tgt = 1.2 * u[T]
+    r2 = 2.0 * (x[T] - tgt)
+    unit = torch.zeros(V, dtype=torch.float64, device=dev)
+    y = torch.empty(V, dtype=torch.float64, device=dev)
+
+    def solve_unit(weights, b):
+        # y = (1 - d) (I - d P^T)^-1 e_b
+        unit.zero_()
+        unit[int(b)] = 1.0
+        sn.pagerank_fwd(weights, unit, d, tol=1e-14, max_iter=4000, keep_tape=False, out=y)
+        return y[T].clone()
+
+    t0 = time.time()
+    dwh = dw.cpu().numpy()
+    dvh = dv.cpu().numpy()
+    xh = x.cpu().numpy()
+    e_rel, e_fd, v_rel, v_fd = [], [], [], []
+    for p in pe:
+        a_, b_ = int(srcv[p]), int(nb[p])
+        orig = float(w[int(p)].item())
+        scale = d * h * xh[a_] / (1.0 - d)
+        w[int(p)] = orig + h
+        dp = solve_unit(w, b_) * scale
+        w[int(p)] = orig - h
+        dm = -solve_unit(w, b_) * scale
+        w[int(p)] = orig
+        fd = float(((dp - dm) * (r2 + dp + dm)).sum().item()) / (2 * h)
+        e_fd.append(fd)
+        e_rel.append(max_rel([dwh[p]], [fd]))
+    for t in pv:
+        yt = solve_unit(w, t)
+        fd = float((yt * r2).sum().item())
+        v_fd.append(fd)
+        v_rel.append(max_rel([dvh[t]], [fd]))
+    r = {"h": h, "edges": len(pe), "vertices": len(pv), "targets": int(T.numel()),
+         "edge_max_rel": max(e_rel), "vertex_max_rel": max(v_rel),
+         "edge_fd_abs_range": [float(np.min(np.abs(e_fd))), float(np.max(np.abs(e_fd)))],
+         "vertex_fd_abs_range": [float(np.min(np.abs(v_fd))), float(np.max(np.abs(v_fd)))],
+         "solves": 2 * len(pe) + len(pv), "seconds": time.time() - t0,
+         "method": "central differences of L over the perturbed fixed points, each solved "
+                   "for its difference from x (tol 1e-14)"}
+    r["ok"] = max(r["edge_max_rel"], r["vertex_max_rel"]) <= 1e-6
+    parity["adjoint_fd_ok"] = r["ok"]
+    parity["adjoint_fd_max_rel"] = max(r["edge_max_rel"], r["vertex_max_rel"])
+    return r
+
+
+def cpu_baseline(hg, spec, roots, args, step_pr, step_lv, ext, parity):
+    """The reference's OpenMP kernels (oracle/_ref) on this host's cores over
+    the same store, one full step (run() time only), and the check of the
+    device step's outputs against them: PageRank max relative error
+    <= 1e-12, every BFS row equal.  The triangle count of the extras is
+    checked against the oracle's count on the reference's own adjacency of
+    the snapshot (lgo_csr_tc)."""
+    from oracle.bind import Reference, csr_triangles, ref_available
     if not ref_available():
         return None
     t0 = time.time()
@@ -761,18 +1026,46 @@ def cpu_baseline(hg, spec, roots, args):
     build_s = time.time() - t0
     deg = R.degrees(-1)
     E = int(deg.sum())
-    _, t_pr = R.pagerank_pull(-1, args.pr_iters, 0.85)
-    t_bfs, reach = 0.0, 0
-    for r in roots:
+    pr_ref, t_pr = R.pagerank_pull(-1, args.pr_iters, 0.85)
+    t_bfs, reach, rows_equal = 0.0, 0, 0
+    for i, r in enumerate(roots):
         lv, t = R.bfs(-1, int(r))
         t_bfs += t
         reach += int(deg[lv < 2147483646].sum(dtype=np.int64))
+        rows_equal += bool(np.array_equal(lv, step_lv[i]))
     gteps = (args.pr_iters * E + reach) / (t_pr + t_bfs) / 1e9
-    return {"value": gteps, "unit": "GTEPS", "cores": Reference.max_threads(),
-            "kind": "reference",
-            "sample": f"one full step (pagerank_double x{args.pr_iters} + sssp_unweighted "
-                      f"BFS from {len(roots)} roots) on the same store, run() time only",
-            "pagerank_s": t_pr, "bfs_s": t_bfs, "store_build_s": build_s}
+    out = {"value": gteps, "unit": "GTEPS", "cores": Reference.max_threads(),
+           "kind": "reference",
+           "sample": f"one full step (pagerank_double x{args.pr_iters} + sssp_unweighted "
+                     f"BFS from {len(roots)} roots) on the same store, run() time only",
+           "pagerank_s": t_pr, "bfs_s": t_bfs, "store_build_s": build_s}
+    if args.no_parity:
+        return out
+    parity["pagerank_max_rel"] = max_rel(step_pr, pr_ref)
+    parity["pagerank_ok"] = parity["pagerank_max_rel"] <= 1e-12
+    parity["bfs_rows_equal"] = f"{rows_equal} of {len(roots)}"
+    parity["bfs_ok"] = rows_equal == len(roots)
+    parity["against"] = ("the reference's pagerank_double and sssp_unweighted (oracle/_ref) "
+                         "on the same store; outputs of the last timed step")
+    tc = (ext or {}).get("main_store", {}).get("triangle_count") if ext else None
+    if tc and "triangles" in tc:
+        t1 = time.time()
+        off, nb = R.adjacency(-1, 0)
+        want, work = csr_triangles(spec.max_nodes, off, nb, with_work=True)
+        del off, nb
+        parity["triangles_gpu"] = tc["triangles"]
+        parity["triangles_oracle"] = want
+        parity["triangles_ok"] = tc["triangles"] == want
+        parity["triangles_oracle_s"] = time.time() - t1
+        # the triangle kernel's byte model: 4 B per list entry read by the
+        # intersections of the degree-oriented edges
+        peak, _ = measured_peak()
+        gbs = 4 * work / (tc["ms"] / 1e3) / 1e9
+        tc["roofline"] = {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                          "frac": gbs / peak, "algorithmic_bytes": 4 * work,
+                          "bytes_model": "sum over degree-oriented edges (u, v) of "
+                                         "4 B x (|N+(u)| + |N+(v)|), counted by the oracle"}
+    return out
 
 
 def barrier(ws):

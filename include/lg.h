@@ -337,14 +337,16 @@ lg_status lg_pagerank_push(lg_snapshot* snap, int iterations, double damping,
 
 /* The same PageRank for callers that cannot let the library allocate device
  * memory (this entry point has no counterpart in the reference).
- * lg_pagerank_pull grows store-owned scratch with cudaMalloc; a thread that is
- * capturing its stream into a CUDA graph may not call cudaMalloc/cudaFree, and
- * a process whose device memory is already handed to another allocator may see
- * cudaMalloc fail or stall.  This variant allocates nothing: its per-iteration
- * vectors live in a fixed LG_NOALLOC_SCRATCH_BYTES area compiled into the
- * library, which every GPU that loads the library keeps reserved until the
- * process exits.  The graph must fit: 24 bytes per vertex plus 16 bytes per
- * 2048 in-CSR slots <= LG_NOALLOC_SCRATCH_BYTES (about 2.7 million vertices),
+ * lg_pagerank_pull grows store-owned scratch with cudaMalloc.  Some hosts
+ * cannot allow that: a serving process whose device memory is handed out
+ * in full to another allocator (a framework's caching allocator or a memory
+ * pool sized to the GPU), where a new cudaMalloc fails or forces a
+ * device-wide synchronisation, or code that has a rule of no allocation once
+ * it has started.  This variant allocates nothing: its per-iteration vectors
+ * live in a fixed LG_NOALLOC_SCRATCH_BYTES area compiled into the library,
+ * which every GPU that loads the library keeps reserved until the process
+ * exits.  The graph must fit: 24 bytes per vertex plus 16 bytes per 1024
+ * in-CSR slots <= LG_NOALLOC_SCRATCH_BYTES (about 2.7 million vertices),
  * otherwise LG_EINVAL.  The first call on each device looks up the area's
  * device address (cudaGetSymbolAddress) with that device current; make that
  * first call before any stream capture.  All calls share the one area and

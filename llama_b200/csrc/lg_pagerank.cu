@@ -19,198 +19,69 @@
 // snapshot's own when lg_snapshot_flatten made one, else one built for the
 // call in store scratch.
 //
-// pr_flat_step gives each warp a tile of kFlatTile consecutive edges, 8 per
-// lane: it issues the tile's id loads and gathers up front, adds each
-// lane's values serially and joins the lanes with one segmented warp scan
-// keyed by the head bits; a vertex that runs past a tile boundary leaves
-// partials (carry_first, carry_last) that pr_flat_fixup adds.  No block
-// barriers: each warp stages its finished row sums in its own shared memory.
-// Vertices without in-edges have the constant rank (1-d)/N after the first
+// pr_flat_step is the flat sweep of lg_flat_sweep.cuh with the PageRank op:
+// each warp takes a tile of kFlatTile consecutive edges, 8 per lane, issues
+// the tile's id loads and gathers up front, adds each lane's values serially
+// and joins the lanes with one segmented warp scan keyed by the head bits; a
+// vertex that runs past a tile boundary leaves partials (carry_first,
+// carry_last) that pr_flat_fixup adds.  No block barriers: each warp stages
+// its finished row sums in its own shared memory.  Vertices without in-edges have the constant rank (1-d)/N after the first
 // iteration and are written once (pr_empty_rows).
 //
 // lg_pagerank_pull_noalloc cannot hold the E-sized flat array, so it walks
 // the fragments directly every iteration (pr_pull_step, one CTA per 1024
 // virtual slots, values staged in shared memory).
-#include "lg_flat.cuh"
+#include "lg_flat_sweep.cuh"
 
 #include <mutex>
 
 namespace lg {
 
 constexpr uint32_t kPrLong = 64;       // entries with more slots are reduced by a warp
-constexpr int kFlatWarps = 8;          // warps (tiles) per CTA of pr_flat_step
 
 // ---------------------------------------------------------------------------
 // Iterations over the flat array
 // ---------------------------------------------------------------------------
 
-struct FlatArgs {
-	const uint32_t* ids;       // E
-	const uint32_t* heads;     // ntiles * kFlatTileWords + 1 words
+// One PageRank iteration as a flat sweep (lg_flat_sweep.cuh): an edge's value
+// is the gathered contribution of its source; a row's sum s gives
+// pr = (1-d)/N + d*s and the next contribution pr / out_degree.
+struct PrOp {
+	static constexpr bool kResidual = false;
 	const uint32_t* nz_rows;   // R
 	const uint32_t* nz_outdeg; // R: out-degree of nz_rows[k]
-	const uint32_t* nz_off;    // R
-	const uint32_t* tile_seg;  // ntiles
-	uint32_t E, R, ntiles;
-	const uint32_t* outdeg;
 	const double* contrib;
 	double* contrib_next;
 	double* pr_out;            // written when non-null (last iteration)
 	double base;               // (1 - d) / N
 	double d;
-	double* carry_first;       // per tile: the part of a row begun before it
-	double* carry_last;        // per tile: the part of a row that runs past it
-};
-
-__device__ __forceinline__ void flat_finish(const FlatArgs& a, uint32_t k, double s) {
-	const uint32_t v = __ldg(a.nz_rows + k);
-	const double pr = __dadd_rn(a.base, __dmul_rn(a.d, s));
-	const uint32_t dg = __ldg(a.nz_outdeg + k);
-	a.contrib_next[v] = dg ? pr / (double)dg : 0.0;
-	if (a.pr_out) a.pr_out[v] = pr;
-}
-
-// One warp per tile of kFlatTile edges; lane j takes the kFlatPerLane
-// consecutive edges e0 + 8j ... e0 + 8j + 7 (two 16-byte id loads) and the
-// matching byte of the tile's head bits.  Each lane adds its values
-// serially: the part before its first head (lead) continues the row open
-// from the lanes to its left, rows that begin and end inside the lane are
-// complete, and the part after its last head (tail) is open to the right.
-// One segmented warp scan over (has head, tail or lead) gives every lane
-// the open row's total so far.  Finished row sums are staged in shared
-// memory and turned into ranks 32 at a time at the end of the tile.
-__global__ void __launch_bounds__(kFlatWarps * 32)
-pr_flat_step(FlatArgs a) {
-	__shared__ double rowsum[kFlatWarps][kFlatTile];
-	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-	const uint32_t t = blockIdx.x * kFlatWarps + wid;
-	if (t >= a.ntiles) return;                       // whole warps leave together
-	double* rs = rowsum[wid];
-	const uint32_t e0 = t * kFlatTile;
-	const uint32_t eb = e0 + lane * kFlatPerLane;    // this lane's first edge
-	const unsigned char* hbytes = reinterpret_cast<const unsigned char*>(a.heads);
-	const uint32_t hb = __ldg(hbytes + (size_t)t * (kFlatTile / 8) + lane);
-	const uint32_t hnext = __ldg(hbytes + (size_t)(t + 1) * (kFlatTile / 8)) & 1u;
-	uint32_t id[kFlatPerLane];
-	if (eb + kFlatPerLane <= a.E) {
-		// one 32-byte load per lane (eb is a multiple of 8), evict-first so
-		// the streamed ids do not push the gathered contributions out of L2
-		asm("ld.global.cs.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-			: "=r"(id[0]), "=r"(id[1]), "=r"(id[2]), "=r"(id[3]),
-			  "=r"(id[4]), "=r"(id[5]), "=r"(id[6]), "=r"(id[7])
-			: "l"(a.ids + eb));
-	} else {
+	__device__ __forceinline__ bool skip() const { return false; }
+	__device__ __forceinline__ void values(uint32_t, const uint32_t (&id)[kFlatPerLane],
+			double (&x)[kFlatPerLane]) const {
 #pragma unroll
 		for (int i = 0; i < kFlatPerLane; i++)
-			id[i] = eb + i < a.E ? __ldcs(a.ids + eb + i) : kNoId;
+			x[i] = id[i] != kNoId ? __ldg(contrib + id[i]) : 0.0;
 	}
-	double x[kFlatPerLane];
-#pragma unroll
-	for (int i = 0; i < kFlatPerLane; i++)
-		x[i] = id[i] != kNoId ? __ldg(a.contrib + id[i]) : 0.0;
+	__device__ __forceinline__ double finish(uint32_t k, double s) const {
+		const uint32_t v = __ldg(nz_rows + k);
+		const double pr = __dadd_rn(base, __dmul_rn(d, s));
+		const uint32_t dg = __ldg(nz_outdeg + k);
+		contrib_next[v] = dg ? pr / (double)dg : 0.0;
+		if (pr_out) pr_out[v] = pr;
+		return 0.0;
+	}
+	__device__ __forceinline__ void residual(double) const {}
+};
 
-	// heads in the lanes to the left
-	const uint32_t nh = __popc(hb);
-	uint32_t before = nh;
-#pragma unroll
-	for (int o = 1; o < 32; o <<= 1) {
-		const uint32_t q = __shfl_up_sync(0xffffffffu, before, o);
-		if (lane >= (uint32_t)o) before += q;
-	}
-	const uint32_t H = __shfl_sync(0xffffffffu, before, 31);   // heads in the tile
-	before -= nh;
-	// serial pass over the lane's values
-	double acc = 0.0, lead = 0.0;
-	uint32_t seen = 0;
-#pragma unroll
-	for (int i = 0; i < kFlatPerLane; i++) {
-		if ((hb >> i) & 1u) {
-			if (seen == 0) lead = acc;
-			else rs[before + seen - 1] = acc;      // a row inside the lane
-			seen++;
-			acc = 0.0;
-		}
-		acc += x[i];
-	}
-	if (seen == 0) lead = acc;
-	// open row total at the end of each lane: scan of (has head, value)
-	bool f = nh != 0;
-	double v = f ? acc : lead;
-#pragma unroll
-	for (int o = 1; o < 32; o <<= 1) {
-		const double pv = __shfl_up_sync(0xffffffffu, v, o);
-		const bool pf = __shfl_up_sync(0xffffffffu, (uint32_t)f, o) != 0u;
-		if (lane >= (uint32_t)o) {
-			if (!f) v = pv + v;
-			f = f || pf;
-		}
-	}
-	// the open row from the left ends at this lane's first head
-	double open_in = __shfl_up_sync(0xffffffffu, v, 1);
-	if (lane == 0) open_in = 0.0;
-	if (nh != 0) {
-		const double s = open_in + lead;
-		if (before == 0) a.carry_first[t] = s;   // began before the tile
-		else rs[before - 1] = s;
-	}
-	// the row open at the end of the tile
-	const double open_out = __shfl_sync(0xffffffffu, v, 31);
-	const bool closes = (uint64_t)e0 + kFlatTile >= a.E || hnext;
-	if (lane == 31u) {
-		if (H == 0) a.carry_first[t] = open_out;
-		else if (closes) rs[H - 1] = open_out;
-		else a.carry_last[t] = open_out;
-	}
-	__syncwarp();
-	const uint32_t done = (H > 0 && !closes) ? H - 1 : H;
-	const uint32_t seg0 = __ldg(a.tile_seg + t);
-	for (uint32_t r = lane; r < done; r += 32u) flat_finish(a, seg0 + r, rs[r]);
+__global__ void __launch_bounds__(kFlatWarps * 32)
+pr_flat_step(FlatTiles a, PrOp op) {
+	__shared__ double rowsum[kFlatWarps][kFlatTile];
+	flat_sweep_tile(a, op, rowsum);
 }
 
-// Rows that cross tile boundaries: boundary t (edge t * kFlatTile) owns the
-// row that crosses it if that row began in tile t - 1; its value is
-// carry_last[t - 1] + carry_first[t] + ... + carry_first[t1], t1 the tile
-// of its last edge.  A warp takes 32 boundaries; rows over more than four
-// tiles are summed by the whole warp.
-__global__ void pr_flat_fixup(FlatArgs a) {
-	const uint32_t lane = threadIdx.x & 31u;
-	const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const uint32_t t = w * 32u + lane + 1u;
-	bool own = false;
-	uint32_t k = 0, t1 = 0;
-	if (t < a.ntiles) {
-		const uint32_t b = t * kFlatTile;
-		const bool head = __ldg(a.heads + t * kFlatTileWords) & 1u;   // bit of edge b
-		const uint32_t S = __ldg(a.tile_seg + t);
-		if (!head && S > 0) {
-			k = S - 1;
-			const uint32_t start = __ldg(a.nz_off + k);
-			if (start + kFlatTile >= b) {
-				const uint32_t end = k + 1 < a.R ? __ldg(a.nz_off + k + 1) : a.E;
-				t1 = (end - 1) / kFlatTile;
-				own = true;
-			}
-		}
-	}
-	if (own && t1 - t < 4) {
-		double s = __ldcg(a.carry_last + t - 1);
-		for (uint32_t x = t; x <= t1; x++) s += __ldcg(a.carry_first + x);
-		flat_finish(a, k, s);
-		own = false;
-	}
-	uint32_t mm = __ballot_sync(0xffffffffu, own);
-	while (mm) {
-		const int src = __ffs(mm) - 1;
-		mm &= mm - 1;
-		const uint32_t tt = __shfl_sync(0xffffffffu, t, src);
-		const uint32_t kk = __shfl_sync(0xffffffffu, k, src);
-		const uint32_t tt1 = __shfl_sync(0xffffffffu, t1, src);
-		double s = 0.0;
-		for (uint32_t x = tt + lane; x <= tt1; x += 32u) s += __ldcg(a.carry_first + x);
-#pragma unroll
-		for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-		if (lane == 0) flat_finish(a, kk, __ldcg(a.carry_last + tt - 1) + s);
-	}
+__global__ void __launch_bounds__(kFixupThreads)
+pr_flat_fixup(FlatTiles a, PrOp op) {
+	flat_sweep_fixup_body(a, op);
 }
 
 // nz_outdeg[k] = out-degree of row k's vertex (rows read it in order).
@@ -413,24 +284,15 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 	const uint32_t ntiles = f->ntiles;
 	const uint32_t* flat_off = f->off.as<uint32_t>();
 
-	FlatArgs a;
-	a.ids = f->ids.as<uint32_t>();
-	a.heads = f->heads();
-	a.nz_rows = f->nz_rows();
-	a.nz_outdeg = f->nz_outdeg.as<uint32_t>();
-	a.nz_off = f->nz_off();
-	a.tile_seg = f->tile_seg();
-	a.E = (uint32_t)f->E;
-	a.R = (uint32_t)f->R;
-	a.ntiles = ntiles;
-	a.outdeg = outdeg;
-	a.base = base;
-	a.d = damping;
 	LG_TRY(sc[0].reserve(V * sizeof(double)));
 	LG_TRY(sc[1].reserve(V * sizeof(double)));
 	LG_TRY(sc[2].reserve(2ull * std::max<uint32_t>(ntiles, 1) * sizeof(double)));
-	a.carry_first = sc[2].as<double>();
-	a.carry_last = a.carry_first + std::max<uint32_t>(ntiles, 1);
+	const FlatTiles a = flat_tiles(*f, sc[2].as<double>());
+	PrOp op;
+	op.nz_rows = f->nz_rows();
+	op.nz_outdeg = f->nz_outdeg.as<uint32_t>();
+	op.base = base;
+	op.d = damping;
 	const bool dev_out = is_device_pointer(ranks);
 	double* pr_buf = ranks;
 	if (!dev_out) {
@@ -443,18 +305,18 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 	pr_empty_rows<<<grid_for(V, B), B, 0, st>>>(flat_off, outdeg, V, base, c1, nullptr);
 	LG_CUDA(cudaGetLastError(), "pr_init");
 	s->launches += 2;
-	const unsigned step_blocks = (ntiles + kFlatWarps - 1) / kFlatWarps;
-	const unsigned fix_blocks = grid_for(ntiles, B);   // a thread per tile boundary
+	const unsigned step_blocks = flat_sweep_blocks(ntiles);
+	const unsigned fix_blocks = flat_fixup_blocks(ntiles);   // a thread per tile boundary
 	for (int it = 0; it < iterations; it++) {
-		a.contrib = (it & 1) ? c1 : c0;
-		a.contrib_next = (it & 1) ? c0 : c1;
-		a.pr_out = (it == iterations - 1) ? pr_buf : nullptr;
+		op.contrib = (it & 1) ? c1 : c0;
+		op.contrib_next = (it & 1) ? c0 : c1;
+		op.pr_out = (it == iterations - 1) ? pr_buf : nullptr;
 		if (ntiles > 0) {
-			pr_flat_step<<<step_blocks, kFlatWarps * 32, 0, st>>>(a);
+			pr_flat_step<<<step_blocks, kFlatWarps * 32, 0, st>>>(a, op);
 			s->launches++;
 		}
 		if (ntiles > 1) {
-			pr_flat_fixup<<<fix_blocks, B, 0, st>>>(a);
+			pr_flat_fixup<<<fix_blocks, kFixupThreads, 0, st>>>(a, op);
 			s->launches++;
 		}
 		if (it == 0 && iterations > 1) {
@@ -480,10 +342,10 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 //
 // lg_pagerank_pull keeps its per-iteration vectors in store-owned scratch
 // that it grows with cudaMalloc.  Some callers cannot have the library
-// allocate: a thread that is capturing work into a CUDA graph (cudaMalloc
-// and cudaFree are not allowed while its stream is being captured), or a
-// process whose device memory is already handed out to another allocator,
-// where a new cudaMalloc can fail or stall on a device-wide synchronisation.
+// allocate: a process whose device memory is already handed out to another
+// allocator (a framework's caching allocator, a pool sized to the GPU),
+// where a new cudaMalloc can fail or stall on a device-wide
+// synchronisation, or serving code that allows no allocation after start-up.
 // For them this variant runs the fragment-walking kernels on a fixed scratch
 // area that is part of the library image: LG_NOALLOC_SCRATCH_BYTES of device
 // memory, reserved on every GPU that loads the library, until the process

@@ -723,3 +723,307 @@ void lgo_ppr(void* gp, int level, const int64_t* seeds, int K, int iters,
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// At-size checks.  The functions below work on plain CSR arrays (offsets +
+// neighbour ids), such as the adjacency the reference's own iterator returns
+// for a snapshot (oracle/_ref), and use OpenMP so that the benchmark's
+// full-size workloads can be checked on the host cores in seconds.  Each is
+// pinned against the serial store-walking function above on small graphs
+// (tests/test_oracle_at_size.py).
+// ---------------------------------------------------------------------------
+
+#include <omp.h>
+#include <parallel/algorithm>
+
+namespace {
+
+inline uint64_t gen_mix64(uint64_t z) {            // splitmix64 finaliser
+	z += 0x9e3779b97f4a7c15ull;
+	z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+	z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+	return z ^ (z >> 31);
+}
+inline double gen_unit(uint64_t h) { return (double)(h >> 11) * (1.0 / 9007199254740992.0); }
+inline uint64_t gen_canon(uint32_t s, uint32_t t, int symmetric) {
+	if (symmetric && t < s) std::swap(s, t);
+	return ((uint64_t)s << 32) | t;
+}
+inline uint32_t gen_scramble(uint64_t x, int scale, uint64_t seed) {
+	const uint64_t mask = (scale >= 64) ? ~0ull : ((1ull << scale) - 1);
+	const uint64_t k1 = gen_mix64(seed ^ 0x1234567ull) | 1ull;
+	const uint64_t k2 = gen_mix64(seed ^ 0x89abcdefull);
+	const uint64_t k3 = gen_mix64(seed ^ 0x13579bdfull) | 1ull;
+	const int half = scale / 2 > 0 ? scale / 2 : 1;
+	x = (x * k1 + k2) & mask;
+	x ^= x >> half;
+	x = (x * k3) & mask;
+	x ^= x >> half;
+	x = (x * k1 + (k2 >> 7)) & mask;
+	return (uint32_t)x;
+}
+
+struct GenLevel { std::vector<uint32_t> src, dst, dsrc, ddst, w; };
+struct Gen { std::vector<GenLevel> lv; };
+
+} // namespace
+
+extern "C" {
+
+// Parameters of a seeded workload, field for field the engine's
+// lg_graph_spec (include/lg_host.h).
+typedef struct lgo_gen_spec {
+	int kind;                  // 0 R-MAT, 1 Kronecker (scrambled ids)
+	int scale;
+	double edge_factor, a, b, c;
+	uint64_t seed;
+	int symmetrize, num_levels;
+	double level0_fraction, delete_fraction;
+	uint64_t split_seed;
+	uint32_t weight_max;
+	uint64_t weight_seed;
+} lgo_gen_spec;
+
+// The benchmark workloads' levels, generated without the engine: R-MAT
+// quadrant recursion on splitmix64 hashes of (seed, draw index), self-loops
+// and duplicates dropped, every edge's insertion level and deletion level
+// decided by hashes of its canonical pair, weights by a hash of the pair.
+// This is the generator specification the engine's host builder
+// implements (lg_hgraph_build); a CPU test checks that both produce the same
+// levels.  Returns a handle, or null on bad parameters.
+void* lgo_gen_create(const lgo_gen_spec* s) {
+	if (!s || s->scale < 1 || s->scale > 31 || s->num_levels < 1 || s->num_levels > 64)
+		return nullptr;
+	const uint64_t V = 1ull << s->scale;
+	const uint64_t draws = (uint64_t)llround(s->edge_factor * (double)V);
+	const uint64_t need = s->symmetrize ? 2 * draws : draws;
+	const double a = s->a, ab = s->a + s->b, abc = s->a + s->b + s->c;
+	const uint64_t SKIP = ~0ull;
+	std::vector<uint64_t> keys(need);
+#pragma omp parallel for schedule(static)
+	for (uint64_t i = 0; i < draws; i++) {
+		uint64_t state = gen_mix64(s->seed * 0x2545f4914f6cdd1dull + i);
+		uint32_t u = 0, v = 0;
+		for (int k = 0; k < s->scale; k++) {
+			state = gen_mix64(state);
+			const double r = gen_unit(state);
+			const uint32_t row = r < ab ? 0u : 1u;
+			const uint32_t col = (r < a || (r >= ab && r < abc)) ? 0u : 1u;
+			u = (u << 1) | row;
+			v = (v << 1) | col;
+		}
+		if (s->kind == 1) {
+			u = gen_scramble(u, s->scale, s->seed);
+			v = gen_scramble(v, s->scale, s->seed);
+		}
+		const bool loop = u == v;
+		keys[i] = loop ? SKIP : (((uint64_t)u << 32) | v);
+		if (s->symmetrize) keys[draws + i] = loop ? SKIP : (((uint64_t)v << 32) | u);
+	}
+	__gnu_parallel::sort(keys.begin(), keys.end());
+	uint64_t n = 0;
+	for (uint64_t i = 0; i < need && keys[i] != SKIP; i++)
+		if (n == 0 || keys[i] != keys[n - 1]) keys[n++] = keys[i];
+	const int L = s->num_levels;
+	const double f0 = s->level0_fraction, p = s->delete_fraction;
+	std::vector<uint8_t> la(n), ld(n);
+#pragma omp parallel for schedule(static)
+	for (uint64_t i = 0; i < n; i++) {
+		const uint32_t u = (uint32_t)(keys[i] >> 32), v = (uint32_t)keys[i];
+		const uint64_t k = gen_canon(u, v, s->symmetrize);
+		const double x = gen_unit(gen_mix64(s->split_seed ^ gen_mix64(k)));
+		int add = 0;
+		if (L > 1 && x >= f0) {
+			add = 1 + (int)((x - f0) / (1.0 - f0) * (double)(L - 1));
+			if (add > L - 1) add = L - 1;
+		}
+		int del = 255;
+		for (int l = add + 1; l < L && p > 0; l++) {
+			const double r = gen_unit(gen_mix64(gen_mix64(s->split_seed + 0x51ed27u * (uint64_t)l) ^ k));
+			if (r < p) { del = l; break; }
+		}
+		la[i] = (uint8_t)add;
+		ld[i] = (uint8_t)del;
+	}
+	Gen* g = new Gen();
+	g->lv.resize(L);
+	for (uint64_t i = 0; i < n; i++) {
+		const uint32_t u = (uint32_t)(keys[i] >> 32), v = (uint32_t)keys[i];
+		GenLevel& A = g->lv[la[i]];
+		A.src.push_back(u);
+		A.dst.push_back(v);
+		if (s->weight_max) {
+			const uint64_t k = gen_canon(u, v, s->symmetrize);
+			A.w.push_back(1u + (uint32_t)(gen_mix64(s->weight_seed ^ gen_mix64(k)) % s->weight_max));
+		}
+		if (ld[i] != 255) { g->lv[ld[i]].dsrc.push_back(u); g->lv[ld[i]].ddst.push_back(v); }
+	}
+	return g;
+}
+
+void lgo_gen_destroy(void* h) { delete (Gen*)h; }
+
+int lgo_gen_num_levels(void* h) { return (int)((Gen*)h)->lv.size(); }
+
+// Pointers to level l's new edges (sorted by (src, dst)), deletions and
+// weights (null when unweighted); valid until lgo_gen_destroy.
+int lgo_gen_level(void* h, int l, const uint32_t** src, const uint32_t** dst, uint64_t* n,
+		const uint32_t** dsrc, const uint32_t** ddst, uint64_t* nd, const uint32_t** w) {
+	Gen* g = (Gen*)h;
+	if (l < 0 || l >= (int)g->lv.size()) return -1;
+	const GenLevel& A = g->lv[l];
+	*src = A.src.data(); *dst = A.dst.data(); *n = A.src.size();
+	*dsrc = A.dsrc.data(); *ddst = A.ddst.data(); *nd = A.dsrc.size();
+	*w = A.w.empty() ? nullptr : A.w.data();
+	return 0;
+}
+
+// Triangle count of the symmetrised, de-duplicated graph given as a
+// directed CSR (what lgo_tc counts from a snapshot, and tc_u on the
+// flattened store, triangle_counting.h:343-470): the undirected adjacency is
+// built, every edge is oriented from the endpoint of lower (degree, id) to
+// the higher one, and each triangle u -> v -> w (with u -> w) is found once:
+// u's oriented list is marked, then every list of its members is probed.
+// *pair_work (may be null) receives the sum over oriented edges (u, v) of
+// |N+(u)| + |N+(v)|, the list lengths a merge intersection reads.
+int64_t lgo_csr_tc(uint64_t V, const uint64_t* off, const uint32_t* nb, uint64_t* pair_work) {
+	std::vector<uint64_t> cnt(V + 1, 0);
+	for (uint64_t u = 0; u < V; u++)
+		for (uint64_t k = off[u]; k < off[u + 1]; k++)
+			if (nb[k] != u) { cnt[u + 1]++; cnt[(uint64_t)nb[k] + 1]++; }
+	for (uint64_t v = 0; v < V; v++) cnt[v + 1] += cnt[v];
+	std::vector<uint32_t> adj(cnt[V]);
+	{
+		std::vector<uint64_t> fill(cnt.begin(), cnt.end() - 1);
+		for (uint64_t u = 0; u < V; u++)
+			for (uint64_t k = off[u]; k < off[u + 1]; k++)
+				if (nb[k] != u) { adj[fill[u]++] = nb[k]; adj[fill[nb[k]]++] = (uint32_t)u; }
+	}
+	std::vector<uint32_t> deg(V);
+#pragma omp parallel for schedule(dynamic, 4096)
+	for (uint64_t v = 0; v < V; v++) {
+		std::sort(adj.begin() + cnt[v], adj.begin() + cnt[v + 1]);
+		deg[v] = (uint32_t)(std::unique(adj.begin() + cnt[v], adj.begin() + cnt[v + 1])
+				- (adj.begin() + cnt[v]));
+	}
+	auto before = [&](uint32_t x, uint32_t y) {
+		return deg[x] < deg[y] || (deg[x] == deg[y] && x < y);
+	};
+	// oriented lists, sorted by id
+	std::vector<uint64_t> oo(V + 1, 0);
+	for (uint64_t v = 0; v < V; v++) {
+		uint64_t c = 0;
+		for (uint64_t k = cnt[v]; k < cnt[v] + deg[v]; k++) c += before((uint32_t)v, adj[k]);
+		oo[v + 1] = oo[v] + c;
+	}
+	std::vector<uint32_t> on(oo[V]);
+#pragma omp parallel for schedule(dynamic, 4096)
+	for (uint64_t v = 0; v < V; v++) {
+		uint64_t p = oo[v];
+		for (uint64_t k = cnt[v]; k < cnt[v] + deg[v]; k++)
+			if (before((uint32_t)v, adj[k])) on[p++] = adj[k];
+	}
+	if (pair_work) {
+		uint64_t W = 0;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(+:W)
+		for (uint64_t u = 0; u < V; u++)
+			for (uint64_t k = oo[u]; k < oo[u + 1]; k++)
+				W += (oo[u + 1] - oo[u]) + (oo[(uint64_t)on[k] + 1] - oo[on[k]]);
+		*pair_work = W;
+	}
+	// count: mark u's oriented list, then look up each list of its members
+	int64_t T = 0;
+#pragma omp parallel reduction(+:T)
+	{
+		std::vector<uint32_t> mark(V, 0);
+#pragma omp for schedule(dynamic, 256)
+		for (uint64_t u = 0; u < V; u++) {
+			const uint32_t stamp = (uint32_t)u + 1;
+			for (uint64_t k = oo[u]; k < oo[u + 1]; k++) mark[on[k]] = stamp;
+			for (uint64_t k = oo[u]; k < oo[u + 1]; k++) {
+				const uint32_t v = on[k];
+				for (uint64_t q = oo[v]; q < oo[v + 1]; q++) T += mark[on[q]] == stamp;
+			}
+		}
+	}
+	return T;
+}
+
+// Personalized PageRank over an in-CSR (lgo_ppr's iteration, all K seeds
+// at once and in parallel over vertices): x0 = e_seed, then `iters` times
+// x'[t] = (1-d) [t == seed] + d * sum_{w in in(t)} x[w] / outdeg[w], the
+// in-neighbours added in the order given, so each column is bit-identical to
+// lgo_ppr's.  out is vertex-major, out[v*K + k].
+void lgo_csr_ppr(uint64_t V, const uint64_t* in_off, const uint32_t* in_nb,
+		const uint32_t* outdeg, const int64_t* seeds, int K, int iters, double d,
+		double* out) {
+	std::vector<double> x(V * K, 0.0), nx(V * K);
+	for (int k = 0; k < K; k++) x[(uint64_t)seeds[k] * K + k] = 1.0;
+	for (int it = 0; it < iters; it++) {
+#pragma omp parallel
+		{
+			std::vector<double> S(K);
+#pragma omp for schedule(dynamic, 4096)
+			for (uint64_t t = 0; t < V; t++) {
+				std::fill(S.begin(), S.end(), 0.0);
+				for (uint64_t q = in_off[t]; q < in_off[t + 1]; q++) {
+					const uint64_t w = in_nb[q];
+					for (int k = 0; k < K; k++) S[k] = S[k] + x[w * K + k] / ((double)outdeg[w]);
+				}
+				for (int k = 0; k < K; k++)
+					nx[t * K + k] = ((int64_t)t == seeds[k] ? (1 - d) : 0.0) + d * S[k];
+			}
+		}
+		x.swap(nx);
+	}
+	std::copy(x.begin(), x.end(), out);
+}
+
+// Brandes betweenness centrality over an out-CSR (lgo_bc's restatement of
+// bc_random_bfs, bc_random.h:55-111), the sources in parallel: each thread
+// runs whole sources with its own level / sigma / delta arrays and its own
+// BC sums, which are added at the end (so the order of the per-source adds
+// differs from lgo_bc's; FP64, within rounding).
+void lgo_csr_bc(uint64_t V, const uint64_t* off, const uint32_t* nb,
+		const int64_t* sources, int n, double* bc) {
+	std::fill(bc, bc + V, 0.0);
+#pragma omp parallel
+	{
+		std::vector<int32_t> lev(V);
+		std::vector<double> sigma(V), delta(V), mine(V, 0.0);
+		std::vector<std::vector<uint32_t>> levels;
+#pragma omp for schedule(dynamic, 1)
+		for (int i = 0; i < n; i++) {
+			const int64_t s = sources[i];
+			std::fill(lev.begin(), lev.end(), -1);
+			std::fill(sigma.begin(), sigma.end(), 0.0);
+			levels.assign(1, std::vector<uint32_t>(1, (uint32_t)s));
+			lev[s] = 0;
+			sigma[s] = 1.0;
+			for (int32_t cur = 0; !levels[cur].empty(); cur++) {
+				levels.emplace_back();
+				for (uint32_t v : levels[cur])
+					for (uint64_t q = off[v]; q < off[v + 1]; q++)
+						if (lev[nb[q]] < 0) { lev[nb[q]] = cur + 1; levels[cur + 1].push_back(nb[q]); }
+				for (uint32_t v : levels[cur])
+					for (uint64_t q = off[v]; q < off[v + 1]; q++)
+						if (lev[nb[q]] == cur + 1) sigma[nb[q]] += sigma[v];
+			}
+			for (int32_t cur = (int32_t)levels.size() - 1; cur >= 0; cur--)
+				for (uint32_t v : levels[cur]) {
+					if ((int64_t)v == s) continue;
+					double S = 0.0;
+					for (uint64_t q = off[v]; q < off[v + 1]; q++) {
+						const uint32_t w = nb[q];
+						if (lev[w] == cur + 1) S = S + sigma[v] / sigma[w] * (1 + delta[w]);
+					}
+					delta[v] = S;
+					mine[v] = mine[v] + delta[v];
+				}
+		}
+#pragma omp critical
+		for (uint64_t v = 0; v < V; v++) bc[v] += mine[v];
+	}
+}
+
+} // extern "C"

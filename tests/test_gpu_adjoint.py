@@ -90,3 +90,25 @@ def test_gradients_match_oracle_and_finite_differences():
                 fd = (loss(sn.pagerank_fwd(w, vp, d, keep_tape=False)[0])
                       - loss(sn.pagerank_fwd(w, vm, d, keep_tape=False)[0])) / (2 * h)
                 assert abs(dv[t] - fd) <= 1e-6 * max(abs(fd), 1e-12) + 1e-12, t
+
+
+def test_iteration_count_and_cutoff_match_oracle():
+    # the solve issues iterations in chunks and stops on the device: it must
+    # stop where a loop that checks every iteration stops, and after exactly
+    # max_iter iterations when tol is out of reach
+    spec, hg, O = setup_graph(11, 6)
+    L = hg.num_levels - 1
+    w, v, _, _ = weights_and_teleport(O, L, 3)
+    with Store() as st:
+        st.ingest(hg)
+        with st.snapshot() as sn:
+            x, _, res = sn.pagerank_fwd(w, v, 0.85, tol=1e-10, keep_tape=False)
+            ox, oit = O.wpr_forward(L, w, v, 0.85, tol=1e-10)
+            assert abs(res.iterations - oit) <= 1
+            assert np.abs(x - ox).sum() < 1e-9
+            for m in (1, 2, 3, 16, 17, 33):
+                xm, _, rm = sn.pagerank_fwd(w, v, 0.85, tol=1e-300, max_iter=m,
+                                            keep_tape=False)
+                oxm, oitm = O.wpr_forward(L, w, v, 0.85, tol=1e-300, max_iter=m)
+                assert rm.iterations == m == oitm
+                assert np.max(np.abs(xm - oxm)) <= 1e-15, m

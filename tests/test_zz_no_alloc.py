@@ -1,8 +1,8 @@
 """PageRank through the entry point that allocates no device memory.
 
 lg_pagerank_pull_noalloc serves callers that must not have the library call
-cudaMalloc (for instance while their stream is being captured into a CUDA
-graph, or when another allocator owns the device memory): it runs on a fixed
+cudaMalloc (for instance a process whose device memory another allocator
+already owns, where a new cudaMalloc fails or stalls): it runs on a fixed
 scratch area compiled into liblg.so.  Its results must equal those of
 lg_pagerank_pull, call after call, although every call reuses the same area.
 This file is collected last on purpose.
