@@ -513,6 +513,24 @@ lg_status lg_pagerank_bwd(lg_adjoint* tape, const double* dldx, double* dldw,
 lg_status lg_adjoint_free(lg_adjoint* tape);
 
 /* ---------------------------------------------------------------------------
+ * Launch parameters (no counterpart in the reference, whose OpenMP kernels
+ * have no launch shapes).  Each GPU has a table of values that the kernels
+ * read when they are launched; lg_tune_set pins one, lg_autotune measures
+ * candidates on a snapshot and keeps the fastest.  Out-of-range values are
+ * rejected with LG_EINVAL; every value gives the same results, only the
+ * speed changes.
+ * ------------------------------------------------------------------------- */
+/* Flat-CSR sweeps (PageRank pull, the adjoint's solves): resident CTAs per
+ * SM of a persistent sweep, each warp looping over 256-edge tiles; 0 = one
+ * CTA per 8 tiles, each warp one tile. */
+#define LG_TUNE_PR_CTAS_PER_SM  0
+#define LG_TUNE_COUNT           1
+#define LG_TUNE_MAX_DEVICES     64
+lg_status lg_tune_get(int device, int key, int64_t* value);
+lg_status lg_tune_set(int device, int key, int64_t value);
+lg_status lg_tune_reset(int device);
+
+/* ---------------------------------------------------------------------------
  * Errors.
  * ------------------------------------------------------------------------- */
 /* Copies the calling thread's last error message (NUL-terminated, truncated

@@ -32,6 +32,9 @@ LG_OUTPUT_ASYNC = 1
 LG_ASYNC_MIN_BYTES = 1 << 20
 LG_GEN_RMAT = 0
 LG_GEN_KRONECKER = 1
+LG_TUNE_PR_CTAS_PER_SM = 0
+LG_TUNE_COUNT = 1
+LG_TUNE_MAX_DEVICES = 64
 
 
 class lg_vt_entry(C.Structure):
@@ -169,6 +172,9 @@ SIGNATURES = [
                                C.POINTER(lg_fixed_point_result)]),
     ("lg_pagerank_bwd", _INT, [_P, _P, _P, _P, C.POINTER(lg_fixed_point_result)]),
     ("lg_adjoint_free", _INT, [_P]),
+    ("lg_tune_get", _INT, [_INT, _INT, C.POINTER(_I64)]),
+    ("lg_tune_set", _INT, [_INT, _INT, _I64]),
+    ("lg_tune_reset", _INT, [_INT]),
     ("lg_last_error", C.c_size_t, [C.c_char_p, C.c_size_t]),
     ("lg_status_string", C.c_char_p, [_INT]),
     ("lg_version", C.c_char_p, []),

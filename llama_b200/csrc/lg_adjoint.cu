@@ -29,6 +29,7 @@
 // while the next one runs.  The result is the one the stop-at-first-
 // residual-below-tol loop gives, with no synchronisation per iteration.
 #include "lg_flat_sweep.cuh"
+#include "lg_tune.h"
 
 #include <cmath>
 
@@ -80,6 +81,13 @@ __global__ void __launch_bounds__(kFlatWarps * 32)
 aff_flat_step(FlatTiles a, AffOp op) {
 	__shared__ double rowsum[kFlatWarps][kFlatTile];
 	flat_sweep_tile(a, op, rowsum);
+}
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kFlatWarps * 32, kMinBlocks)
+aff_flat_loop(FlatTiles a, AffOp op) {
+	__shared__ double rowsum[kFlatWarps][kFlatTile];
+	flat_sweep_loop(a, op, rowsum);
 }
 
 __global__ void __launch_bounds__(kFixupThreads)
@@ -346,6 +354,9 @@ lg_status fixed_point(lg_snapshot* sn, const FlatCsr& f, const double* w, const 
 	op.tol = tol;
 	op.E = (uint32_t)f.E;
 	const uint32_t* off = f.off.as<uint32_t>();
+	const int ctas = (int)tune_value(s->device, LG_TUNE_PR_CTAS_PER_SM);
+	int sms = 148;
+	if (ctas > 0) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
 	aff_empty_rows<<<grid_for(V, 256), 256, 0, st>>>(off, V, base, A, B, resid);
 	s->launches++;
 	int done = -1;          // iterations after which the residual fell below tol
@@ -370,7 +381,8 @@ lg_status fixed_point(lg_snapshot* sn, const FlatCsr& f, const double* w, const 
 			op.resid = resid + it;
 			op.prev = it > 0 ? resid + it - 1 : nullptr;
 			if (f.ntiles > 0) {
-				aff_flat_step<<<flat_sweep_blocks(f.ntiles), kFlatWarps * 32, 0, st>>>(a, op);
+				launch_flat_sweep(a, op, sms, ctas, st, aff_flat_step, aff_flat_loop<4>,
+						aff_flat_loop<6>, aff_flat_loop<8>);
 				s->launches++;
 			}
 			if (f.ntiles > 1) {

@@ -62,15 +62,12 @@ inline FlatTiles flat_tiles(const FlatCsr& f, double* carries) {
 // One segmented warp scan over (has head, tail or lead) gives every lane the
 // open row's total so far.
 //
-// This is the body of a kernel launched with kFlatWarps * 32 threads per
-// CTA; rowsum is the CTA's shared double[kFlatWarps][kFlatTile].
+// Processes tile t with the calling warp (rs: the warp's kFlatTile doubles
+// of shared memory) and returns the lane's residual terms.
 template <class Op>
-__device__ __forceinline__ void flat_sweep_tile(const FlatTiles& a, const Op& op,
-		double (*rowsum)[kFlatTile]) {
-	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-	const uint32_t t = blockIdx.x * kFlatWarps + wid;
-	if (t >= a.ntiles || op.skip()) return;          // whole warps leave together
-	double* rs = rowsum[wid];
+__device__ __forceinline__ double flat_sweep_one(const FlatTiles& a, const Op& op, double* rs,
+		uint32_t t) {
+	const uint32_t lane = threadIdx.x & 31u;
 	const uint32_t e0 = t * kFlatTile;
 	const uint32_t eb = e0 + lane * kFlatPerLane;    // this lane's first edge
 	const unsigned char* hbytes = reinterpret_cast<const unsigned char*>(a.heads);
@@ -149,11 +146,46 @@ __device__ __forceinline__ void flat_sweep_tile(const FlatTiles& a, const Op& op
 	const uint32_t seg0 = __ldg(a.tile_seg + t);
 	double res = 0.0;
 	for (uint32_t r = lane; r < done; r += 32u) res += op.finish(seg0 + r, rs[r]);
+	return res;
+}
+
+template <class Op>
+__device__ __forceinline__ void flat_sweep_residual(const Op& op, double res) {
 	if (Op::kResidual) {
 #pragma unroll
 		for (int o = 16; o > 0; o >>= 1) res += __shfl_xor_sync(0xffffffffu, res, o);
-		if (lane == 0 && res != 0.0) op.residual(res);
+		if ((threadIdx.x & 31u) == 0 && res != 0.0) op.residual(res);
 	}
+}
+
+// Body of a kernel launched with kFlatWarps * 32 threads per CTA and one
+// CTA per kFlatWarps tiles: warp w of CTA b takes tile b * kFlatWarps + w.
+// rowsum is the CTA's shared double[kFlatWarps][kFlatTile].
+template <class Op>
+__device__ __forceinline__ void flat_sweep_tile(const FlatTiles& a, const Op& op,
+		double (*rowsum)[kFlatTile]) {
+	const uint32_t wid = threadIdx.x >> 5;
+	const uint32_t t = blockIdx.x * kFlatWarps + wid;
+	if (t >= a.ntiles || op.skip()) return;          // whole warps leave together
+	flat_sweep_residual(op, flat_sweep_one(a, op, rowsum[wid], t));
+}
+
+// The persistent form: a grid of a few CTAs per SM whose warps loop over the
+// tiles (warp w of CTA b: tiles b * kFlatWarps + w, then every gridDim.x *
+// kFlatWarps further), so no warp slot idles while a CTA waits for its
+// slowest warp.
+template <class Op>
+__device__ __forceinline__ void flat_sweep_loop(const FlatTiles& a, const Op& op,
+		double (*rowsum)[kFlatTile]) {
+	if (op.skip()) return;
+	const uint32_t wid = threadIdx.x >> 5;
+	const uint32_t stride = gridDim.x * kFlatWarps;
+	double res = 0.0;
+	for (uint32_t t = blockIdx.x * kFlatWarps + wid; t < a.ntiles; t += stride) {
+		res += flat_sweep_one(a, op, rowsum[wid], t);
+		__syncwarp();                     // rowsum is reused by the next tile
+	}
+	flat_sweep_residual(op, res);
 }
 
 // Rows that cross tile boundaries: boundary t (edge t * kFlatTile) owns the
@@ -215,7 +247,31 @@ __device__ __forceinline__ void flat_sweep_fixup_body(const FlatTiles& a, const 
 inline unsigned flat_sweep_blocks(uint32_t ntiles) {
 	return (ntiles + kFlatWarps - 1) / kFlatWarps;
 }
+// Persistent grid: ctas_per_sm CTAs on each of sms SMs, never more CTAs
+// than tiles need.
+inline unsigned flat_loop_blocks(uint32_t ntiles, int sms, int ctas_per_sm) {
+	const uint64_t g = (uint64_t)sms * (uint64_t)ctas_per_sm;
+	const unsigned need = flat_sweep_blocks(ntiles);
+	return (unsigned)(g < need ? g : need);
+}
 constexpr unsigned kFixupThreads = 256;
+
+// A sweep launcher: the tile kernel (one CTA per kFlatWarps tiles) when
+// ctas_per_sm is 0, else the persistent loop kernel whose register cap
+// allows that many resident CTAs (4, 6 or 8), on that many CTAs per SM.
+template <class Op, class TileK, class LoopK4, class LoopK6, class LoopK8>
+inline void launch_flat_sweep(const FlatTiles& a, const Op& op, int sms, int ctas_per_sm,
+		cudaStream_t st, TileK tile_k, LoopK4 loop4, LoopK6 loop6, LoopK8 loop8) {
+	if (a.ntiles == 0) return;
+	if (ctas_per_sm <= 0) {
+		tile_k<<<flat_sweep_blocks(a.ntiles), kFlatWarps * 32, 0, st>>>(a, op);
+		return;
+	}
+	const unsigned g = flat_loop_blocks(a.ntiles, sms, ctas_per_sm);
+	if (ctas_per_sm <= 4) loop4<<<g, kFlatWarps * 32, 0, st>>>(a, op);
+	else if (ctas_per_sm <= 6) loop6<<<g, kFlatWarps * 32, 0, st>>>(a, op);
+	else loop8<<<g, kFlatWarps * 32, 0, st>>>(a, op);
+}
 inline unsigned flat_fixup_blocks(uint32_t ntiles) { return grid_for(ntiles, kFixupThreads); }
 
 } // namespace lg

@@ -32,6 +32,7 @@
 // the fragments directly every iteration (pr_pull_step, one CTA per 1024
 // virtual slots, values staged in shared memory).
 #include "lg_flat_sweep.cuh"
+#include "lg_tune.h"
 
 #include <mutex>
 
@@ -77,6 +78,13 @@ __global__ void __launch_bounds__(kFlatWarps * 32)
 pr_flat_step(FlatTiles a, PrOp op) {
 	__shared__ double rowsum[kFlatWarps][kFlatTile];
 	flat_sweep_tile(a, op, rowsum);
+}
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kFlatWarps * 32, kMinBlocks)
+pr_flat_loop(FlatTiles a, PrOp op) {
+	__shared__ double rowsum[kFlatWarps][kFlatTile];
+	flat_sweep_loop(a, op, rowsum);
 }
 
 __global__ void __launch_bounds__(kFixupThreads)
@@ -305,14 +313,17 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 	pr_empty_rows<<<grid_for(V, B), B, 0, st>>>(flat_off, outdeg, V, base, c1, nullptr);
 	LG_CUDA(cudaGetLastError(), "pr_init");
 	s->launches += 2;
-	const unsigned step_blocks = flat_sweep_blocks(ntiles);
 	const unsigned fix_blocks = flat_fixup_blocks(ntiles);   // a thread per tile boundary
+	const int ctas = (int)tune_value(s->device, LG_TUNE_PR_CTAS_PER_SM);
+	int sms = 148;
+	if (ctas > 0) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
 	for (int it = 0; it < iterations; it++) {
 		op.contrib = (it & 1) ? c1 : c0;
 		op.contrib_next = (it & 1) ? c0 : c1;
 		op.pr_out = (it == iterations - 1) ? pr_buf : nullptr;
 		if (ntiles > 0) {
-			pr_flat_step<<<step_blocks, kFlatWarps * 32, 0, st>>>(a, op);
+			launch_flat_sweep(a, op, sms, ctas, st, pr_flat_step, pr_flat_loop<4>,
+					pr_flat_loop<6>, pr_flat_loop<8>);
 			s->launches++;
 		}
 		if (ntiles > 1) {

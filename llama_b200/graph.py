@@ -265,6 +265,24 @@ class Tape:
     __del__ = close
 
 
+TUNABLES = {"pr_ctas_per_sm": _lib.LG_TUNE_PR_CTAS_PER_SM}
+
+
+def tune_set(device, name, value):
+    """Pin launch parameter `name` (a TUNABLES key) of a GPU (lg_tune_set)."""
+    check(lib.lg_tune_set(int(device), TUNABLES[name], int(value)))
+
+
+def tune_get(device, name):
+    v = C.c_int64()
+    check(lib.lg_tune_get(int(device), TUNABLES[name], C.byref(v)))
+    return v.value
+
+
+def tune_reset(device):
+    check(lib.lg_tune_reset(int(device)))
+
+
 def ppr(snapshots, seeds, iterations=20, damping=0.85, out=None):
     """Personalized PageRank (``lg_ppr``) for len(seeds) seeds on every
     snapshot in one captured graph; returns [n_snaps, max_nodes, K]."""

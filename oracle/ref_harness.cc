@@ -134,13 +134,22 @@ int llref_add_level_weighted(void* gp, const uint32_t* src, const uint32_t* dst,
 	int r = llref_add_level(gp, src, dst, n, dsrc, ddst, nd);
 	if (r) return r;
 	g->weight->cow_init_level(G.out().max_edges(level));
-	for (uint64_t i = 0; i < n; i++) {
-		edge_t e = G.out().find(src[i], dst[i]);
-		if (e == LL_NIL_EDGE || LL_EDGE_LEVEL(e) != (size_t)level) return -4;
-		float f = (float)w[i];
-		uint32_t bits;
-		memcpy(&bits, &f, 4);
-		g->weight->cow_write(e, bits);
+	// A vertex's new edges are the first fragment its iteration yields and
+	// sit at consecutive edge ids in input order, so each vertex needs one
+	// find (which returns at once) for its first new edge.
+	for (uint64_t i = 0; i < n; ) {
+		uint64_t j = i;
+		while (j < n && src[j] == src[i]) j++;
+		const edge_t e0 = G.out().find(src[i], dst[i]);
+		if (e0 == LL_NIL_EDGE || LL_EDGE_LEVEL(e0) != (size_t)level) return -4;
+		for (uint64_t k = i; k < j; k++) {
+			const edge_t e = e0 + (edge_t)(k - i);
+			float f = (float)w[k];
+			uint32_t bits;
+			memcpy(&bits, &f, 4);
+			g->weight->cow_write(e, bits);
+		}
+		i = j;
 	}
 	g->weight->cow_finish_level();
 	return 0;

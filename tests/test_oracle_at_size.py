@@ -101,3 +101,24 @@ def test_csr_from_edges_keeps_order():
     off, nb = csr_from_edges(4, src, dst)
     assert off.tolist() == [0, 2, 3, 5, 5]
     assert nb.tolist() == [6, 9, 8, 5, 7]
+
+
+@pytest.mark.skipif(not __import__("oracle.bind", fromlist=["ref_available"]).ref_available(),
+                    reason="oracle/_ref not built")
+def test_reference_weighted_levels_match_the_oracle():
+    # the reference harness writes each vertex's new-edge weights by edge id
+    # from the vertex's first new edge; its sssp_weighted must see the
+    # weights the oracle stores per slot
+    from oracle.bind import Reference
+    spec = SPECS[2]
+    lv = generate_levels(**spec_params(spec))
+    R = Reference(spec.max_nodes)
+    O = Oracle(spec.max_nodes)
+    for x in lv:
+        R.add_level(*x)
+        O.add_level(*x)
+    L = len(lv) - 1
+    for r in workloads.pick_roots(O.degrees(L, 0), 4, seed=9):
+        want, _ = O.sssp(L, int(r))
+        got, _ = R.sssp(-1, int(r))
+        assert np.array_equal(got, want)
