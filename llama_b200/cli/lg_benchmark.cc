@@ -97,7 +97,10 @@ bool read_level(const char* path, Level& lv, uint64_t& max_id) {
 void usage() {
 	fprintf(stderr,
 		"Usage: lg_benchmark [-r TASK] [-R ROOT] [-n ITERS] [-l LEVELS] [-c COUNT]\n"
-		"                    [-o FILE] [-k K] [-s SEED] [-d DEV] (-G rmat:S:L:SEED | FILE...)\n"
+		"                    [-o FILE] [-k K] [-s SEED] [-d DEV] [-N MAX_NODES]\n"
+		"                    (-G rmat:S:L:SEED | FILE...)\n"
+		"-N: vertices of the store (at least the largest id in the files + 1; the\n"
+		"    reference's max_nodes, which PageRank's N counts)\n"
 		"Tasks: pagerank_double pagerank pagerank_double_push bfs_count sssp_unweighted\n"
 		"       sssp_weighted tc_u tarjan_scc bc_random ppr\n");
 }
@@ -117,9 +120,10 @@ int main(int argc, char** argv) {
 	std::string task = "pagerank_double", out_file, gen;
 	long long root = 0;
 	int iters = 10, max_levels = -1, count = 1, device = 0, k = -1;
+	unsigned long long min_nodes = 0;
 	unsigned seed = 1;
 	int c;
-	while ((c = getopt(argc, argv, "r:R:n:l:c:o:k:s:G:d:h")) != -1) {
+	while ((c = getopt(argc, argv, "r:R:n:l:c:o:k:s:G:d:N:h")) != -1) {
 		switch (c) {
 		case 'r': task = optarg; break;
 		case 'R': root = atoll(optarg); break;
@@ -131,6 +135,7 @@ int main(int argc, char** argv) {
 		case 's': seed = (unsigned)atoi(optarg); break;
 		case 'G': gen = optarg; break;
 		case 'd': device = atoi(optarg); break;
+		case 'N': min_nodes = strtoull(optarg, nullptr, 10); break;
 		default: usage(); return c == 'h' ? 0 : 1;
 		}
 	}
@@ -161,7 +166,8 @@ int main(int argc, char** argv) {
 		for (size_t i = 0; i < files.size(); i++)
 			if (!read_level(files[i].c_str(), lv[i], max_id)) return 1;
 		for (auto& l : lv) weighted |= l.weighted;
-		CHECK(lg_hgraph_create(&g, max_id + 1, 1), "lg_hgraph_create");
+		CHECK(lg_hgraph_create(&g, std::max<uint64_t>(max_id + 1, min_nodes), 1),
+				"lg_hgraph_create");
 		for (auto& l : lv)
 			CHECK(lg_hgraph_add_level(g, l.src.data(), l.dst.data(), l.src.size(),
 					l.dsrc.data(), l.ddst.data(), l.dsrc.size(),

@@ -345,17 +345,13 @@ def test_cli_return_value_matches_reference(golden, tmp_path, task):
     L = len(files) - 1
     V = int(golden["V"])
     root = int(golden["roots"][0])
-    # the CLI sizes the store by the largest id in the files; isolated
-    # trailing vertices change N for PageRank, so compare only when equal
-    used = max(int(x.max()) for lv in golden["levels"] for x in lv[:4] if len(x)) + 1
-    if root >= used:
-        pytest.skip("root is an isolated trailing vertex")
-    out = subprocess.run([exe, "-r", task, "-R", str(root), "-n", str(int(golden["pr_iters"]))]
-                         + files, capture_output=True, text=True, check=True).stdout
+    # -N gives the store the fixture's max_nodes (trailing isolated vertices
+    # included), the N of the reference's PageRank
+    out = subprocess.run([exe, "-r", task, "-R", str(root), "-n", str(int(golden["pr_iters"])),
+                          "-N", str(V)] + files,
+                         capture_output=True, text=True, check=True).stdout
     ret = float(out.strip().splitlines()[-1].split(":")[1])
     if task in ("pagerank_double", "pagerank_double_push"):
-        if used != V:
-            pytest.skip("largest vertex id is isolated")
         key = "pr" if task == "pagerank_double" else "prpush"
         assert abs(ret - float(np.sum(golden[f"{key}{L}"]))) <= 1e-9
     elif task == "bfs_count":
