@@ -75,6 +75,9 @@ def parse():
     p.add_argument("--fd-probes", type=int, default=64,
                    help="edges and vertices probed by finite differences (each)")
     p.add_argument("--workload", default="c2", choices=["c2", "c5"])
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the default launch parameters instead of measuring them "
+                        "(lg_autotune) before the warm-up")
     p.add_argument("--no-parity", action="store_true",
                    help="skip the checks of the outputs against the reference / oracle")
     p.add_argument("--traffic", type=float, default=None,
@@ -365,6 +368,13 @@ def run_lg(args):
     roots = workloads.pick_roots(deg, args.roots, seed=3)
     E = sn.num_edges
     ins = sn.stats(1)
+    # launch parameters measured on this snapshot before the warm-up (the
+    # flat sweep's grid, the bottom-up hub threshold, the SSSP ranges)
+    tuning = None
+    if not args.no_autotune:
+        t0 = time.time()
+        tuning = sn.autotune(["pr_ctas_per_sm", "ms_heavy", "sssp_range"])
+        tuning["seconds"] = time.time() - t0
 
     pr_dev = torch.empty(V, dtype=torch.float64, device=f"cuda:{local}")
     lv_dev = torch.empty((len(roots), V), dtype=torch.int32, device=f"cuda:{local}")
@@ -524,7 +534,8 @@ def run_lg(args):
                       "host_build_s": build_s, "ingest_s": ingest_s,
                       "device_bytes": st.device_bytes},
             "roofline": roofline, "bfs_roofline": bfs_roofline, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk, "cpu_baseline": cpu, "parity": parity, "extras": ext}
+            "clocks": clk, "cpu_baseline": cpu, "parity": parity, "tuning": tuning,
+            "extras": ext}
     if rank == 0:
         emit(line, args)
     if sn is not None:
@@ -799,6 +810,8 @@ def extras(args, st, stream, device, parity):
             try:
                 sn = snaps[-1]
                 V, E = sn.max_nodes, sn.num_edges
+                tuned = None if args.no_autotune else sn.autotune(["ppr_ktile", "ppr_range",
+                                                                   "ms_heavy"])
                 src = workloads.pick_roots(sn.out_degrees(), args.bc_sources, seed=14)
                 bc = torch.empty(V, dtype=torch.float64, device=dev)
                 sn.bc(src[:64], batched=True, out=bc)
@@ -832,6 +845,7 @@ def extras(args, st, stream, device, parity):
                 _, tq = _timed(stream, lambda: ppr(snaps, seeds, iterations=20, out=out_ppr))
                 e_all = sum(s.num_edges for s in snaps)
                 K = 256
+                res["tuning"] = tuned
                 res["ppr"] = {"K": K, "iterations": 20, "snapshots": 4, "ms": tq,
                               "gteps": 20 * e_all * K / (tq / 1e3) / 1e9,
                               "roofline": roof(20 * (e_all * (4 + 8 * K) + 4 * 2 * 8 * K * V), tq,

@@ -524,11 +524,40 @@ lg_status lg_adjoint_free(lg_adjoint* tape);
  * SM of a persistent sweep, each warp looping over 256-edge tiles; 0 = one
  * CTA per 8 tiles, each warp one tile. */
 #define LG_TUNE_PR_CTAS_PER_SM  0
-#define LG_TUNE_COUNT           1
+/* Personalized PageRank: columns per pass (a multiple of 32; the K columns
+ * run in passes of this many, each pass all iterations), default 256. */
+#define LG_TUNE_PPR_KTILE       1
+/* Personalized PageRank: in-CSR slots per warp range, default 2048. */
+#define LG_TUNE_PPR_RANGE       2
+/* Delta-stepping SSSP: queue slots per warp range, default 1024. */
+#define LG_TUNE_SSSP_RANGE      3
+/* Multi-source BFS and batched BC bottom-up steps: in-degree above which a
+ * warp, not a thread, scans a vertex's in-edges, default 512. */
+#define LG_TUNE_MS_HEAVY        4
+#define LG_TUNE_COUNT           5
 #define LG_TUNE_MAX_DEVICES     64
 lg_status lg_tune_get(int device, int key, int64_t* value);
 lg_status lg_tune_set(int device, int key, int64_t value);
 lg_status lg_tune_reset(int device);
+
+/* The autotuner: for every tunable whose bit (1u << key) is set in `keys`,
+ * sets each candidate value on the snapshot's GPU in turn, times the call
+ * that reads it on this snapshot (a warm-up call, then the median of three
+ * timed with CUDA events; PageRank pull, PPR with 256 seeds, SSSP and
+ * multi-source BFS from vertices of the snapshot), and keeps the fastest.
+ * Tunables that the snapshot cannot exercise (SSSP without weights, the
+ * others without an in-CSR) are skipped, and so are the PPR ones when three
+ * max_nodes x 256 FP64 blocks do not fit in half of the free device memory.  trials (may be NULL)
+ * receives one entry per candidate measured, up to max_trials; n_trials the
+ * count.  Allocates its own probe buffers; the snapshot is not changed. */
+typedef struct lg_tune_trial {
+	int32_t key;
+	int32_t chosen;    /* 1 for the value kept */
+	int64_t value;
+	double  ms;        /* median time of the probe call */
+} lg_tune_trial;
+lg_status lg_autotune(lg_snapshot* snap, unsigned keys, lg_tune_trial* trials,
+		int max_trials, int* n_trials);
 
 /* ---------------------------------------------------------------------------
  * Errors.

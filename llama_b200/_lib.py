@@ -33,7 +33,11 @@ LG_ASYNC_MIN_BYTES = 1 << 20
 LG_GEN_RMAT = 0
 LG_GEN_KRONECKER = 1
 LG_TUNE_PR_CTAS_PER_SM = 0
-LG_TUNE_COUNT = 1
+LG_TUNE_PPR_KTILE = 1
+LG_TUNE_PPR_RANGE = 2
+LG_TUNE_SSSP_RANGE = 3
+LG_TUNE_MS_HEAVY = 4
+LG_TUNE_COUNT = 5
 LG_TUNE_MAX_DEVICES = 64
 
 
@@ -107,6 +111,11 @@ class lg_snapshot_stats(C.Structure):
                 ("deletions", C.c_uint64)]
 
 
+class lg_tune_trial(C.Structure):
+    _fields_ = [("key", C.c_int32), ("chosen", C.c_int32), ("value", C.c_int64),
+                ("ms", C.c_double)]
+
+
 class lg_graph_spec(C.Structure):
     _fields_ = [("kind", C.c_int), ("scale", C.c_int), ("edge_factor", C.c_double),
                 ("a", C.c_double), ("b", C.c_double), ("c", C.c_double),
@@ -175,6 +184,7 @@ SIGNATURES = [
     ("lg_tune_get", _INT, [_INT, _INT, C.POINTER(_I64)]),
     ("lg_tune_set", _INT, [_INT, _INT, _I64]),
     ("lg_tune_reset", _INT, [_INT]),
+    ("lg_autotune", _INT, [_P, C.c_uint, C.POINTER(lg_tune_trial), _INT, C.POINTER(_INT)]),
     ("lg_last_error", C.c_size_t, [C.c_char_p, C.c_size_t]),
     ("lg_status_string", C.c_char_p, [_INT]),
     ("lg_version", C.c_char_p, []),

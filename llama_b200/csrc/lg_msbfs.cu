@@ -23,6 +23,7 @@
 // 64 sources per pass (see the section below).
 #include "lg_expand.cuh"
 #include "lg_flat.cuh"
+#include "lg_tune.h"
 
 namespace lg {
 
@@ -104,15 +105,15 @@ ms_top_down(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t ql
 // Bottom-up over a flat in-CSR: a thread takes kMsVerts vertices (blockDim
 // apart) and ORs cur[] over kMsChunk in-neighbours of each per round until
 // every root that has not reached the vertex is found, or the list ends.
-// Vertices with more than kMsHeavy in-edges are left to ms_bottom_up_heavy,
-// so no thread walks a hub's list alone.  One vertex and eight neighbours
+// Vertices with more than `heavy` in-edges (LG_TUNE_MS_HEAVY, 512 by
+// default) are left to ms_bottom_up_heavy, so no thread walks a hub's list
+// alone.  One vertex and eight neighbours
 // per round measured best at R-MAT scale 24 (16-root BFS 3.56 ms, against
 // 3.66 for two vertices x 4, 3.93 for four x 4 and for two x 8).
 constexpr int kMsVerts = 1;
-constexpr uint32_t kMsHeavy = 512;
 __global__ void __launch_bounds__(kMsThreads)
 ms_bottom_up_flat(const uint32_t* off, const uint32_t* ids, uint32_t V, u64 lanes,
-		const u64* cur, const u64* seen, u64* nxt) {
+		const u64* cur, const u64* seen, u64* nxt, uint32_t heavy) {
 	const uint32_t base = blockIdx.x * (uint32_t)(kMsThreads * kMsVerts) + threadIdx.x;
 	uint32_t k[kMsVerts], end[kMsVerts];
 	u64 need[kMsVerts], got[kMsVerts];
@@ -125,7 +126,7 @@ ms_bottom_up_flat(const uint32_t* off, const uint32_t* ids, uint32_t V, u64 lane
 			if (need[j]) {
 				k[j] = __ldg(off + v);
 				end[j] = __ldg(off + v + 1);
-				if (end[j] - k[j] > kMsHeavy) { end[j] = k[j]; need[j] = 0; }
+				if (end[j] - k[j] > heavy) { end[j] = k[j]; need[j] = 0; }
 			}
 		}
 	}
@@ -161,11 +162,11 @@ ms_bottom_up_flat(const uint32_t* off, const uint32_t* ids, uint32_t V, u64 lane
 	}
 }
 
-// Vertices of a flat in-CSR with more than kMsHeavy in-edges.
+// Vertices of a flat in-CSR with more than `heavy` in-edges.
 __global__ void ms_heavy_list(const uint32_t* off, uint32_t V, uint32_t* list,
-		unsigned long long* n) {
+		unsigned long long* n, uint32_t heavy) {
 	const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	const bool h = v < V && __ldg(off + v + 1) - __ldg(off + v) > kMsHeavy;
+	const bool h = v < V && __ldg(off + v + 1) - __ldg(off + v) > heavy;
 	ms_push(h, (uint32_t)v, list, n);
 }
 
@@ -529,16 +530,16 @@ lg_status grow_keep(DevBuf& b, size_t need, size_t keep, cudaStream_t st) {
 	return LG_OK;
 }
 
-// The vertices of flat in-CSR f with more than kMsHeavy in-edges, listed in
+// The vertices of flat in-CSR f with more than `heavy` in-edges, listed in
 // buf (a device counter, then the ids) for ms_bottom_up_heavy.
-lg_status heavy_list(lg_store* s, const FlatCsr* f, uint64_t V, DevBuf& buf,
+lg_status heavy_list(lg_store* s, const FlatCsr* f, uint64_t V, uint32_t heavy, DevBuf& buf,
 		uint32_t** list, unsigned long long** count) {
 	LG_TRY(buf.reserve(sizeof(unsigned long long) + std::max<uint64_t>(V, 1) * sizeof(uint32_t)));
 	*count = buf.as<unsigned long long>();
 	*list = reinterpret_cast<uint32_t*>(*count + 1);
 	LG_CUDA(cudaMemsetAsync(*count, 0, sizeof(unsigned long long), s->stream), "clear");
 	ms_heavy_list<<<grid_for(V, 256), 256, 0, s->stream>>>(f->off.as<uint32_t>(), (uint32_t)V,
-			*list, *count);
+			*list, *count, heavy);
 	LG_CUDA(cudaGetLastError(), "ms_heavy_list");
 	s->launches++;
 	return LG_OK;
@@ -602,7 +603,8 @@ extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int 
 	const double alpha = 14.0, beta = 24.0;
 	uint32_t* hlist = nullptr;
 	unsigned long long* hcount = nullptr;
-	if (fi) LG_TRY(heavy_list(s, fi, V, sc[10], &hlist, &hcount));
+	const uint32_t heavy = (uint32_t)tune_value(s->device, LG_TUNE_MS_HEAVY);
+	if (fi) LG_TRY(heavy_list(s, fi, V, heavy, sc[10], &hlist, &hcount));
 
 	for (int p0 = 0; p0 < n_sources; p0 += kMsMaxRoots) {
 		const int n = std::min(kMsMaxRoots, n_sources - p0);
@@ -659,7 +661,7 @@ extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int 
 				if (fi) {
 					ms_bottom_up_flat<<<grid_for(V, kMsThreads * kMsVerts), kMsThreads, 0, st>>>(
 							fi->off.as<uint32_t>(), fi->ids.as<uint32_t>(), (uint32_t)V, lanes,
-							lk, seen, nxt);
+							lk, seen, nxt, heavy);
 					ms_bottom_up_heavy<<<grid, kMsThreads, 0, st>>>(fi->off.as<uint32_t>(),
 							fi->ids.as<uint32_t>(), hlist, hcount, lanes, lk, seen, nxt);
 					s->launches++;
@@ -761,7 +763,8 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 	const double alpha = 14.0, beta = 24.0;
 	uint32_t* hlist = nullptr;
 	unsigned long long* hcount = nullptr;
-	if (fi) LG_TRY(heavy_list(s, fi, V, sc[10], &hlist, &hcount));
+	const uint32_t heavy = (uint32_t)tune_value(s->device, LG_TUNE_MS_HEAVY);
+	if (fi) LG_TRY(heavy_list(s, fi, V, heavy, sc[10], &hlist, &hcount));
 
 	ms_fill<<<(unsigned)sms * 16u, B, 0, st>>>(lv, (uint64_t)n_roots * V);
 	LG_CUDA(cudaGetLastError(), "ms_fill");
@@ -820,7 +823,7 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 				if (fi) {
 					ms_bottom_up_flat<<<grid_for(V, kMsThreads * kMsVerts), kMsThreads, 0, st>>>(
 							fi->off.as<uint32_t>(), fi->ids.as<uint32_t>(), (uint32_t)V, lanes,
-							cur, seen, nxt);
+							cur, seen, nxt, heavy);
 					ms_bottom_up_heavy<<<td_blocks, kMsThreads, 0, st>>>(fi->off.as<uint32_t>(),
 							fi->ids.as<uint32_t>(), hlist, hcount, lanes, cur, seen, nxt);
 					s->launches++;

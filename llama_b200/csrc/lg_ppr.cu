@@ -12,17 +12,20 @@
 // the in-CSR slot space; inside a chunk the 32 edges are handled one after
 // another by the whole warp (the edge id is loaded once for K columns).
 // Rows of vertices that straddle ranges are combined in range order by
-// ppr_fixup.  Every snapshot's iterations are captured into one CUDA graph
+// ppr_fixup.  The K columns are processed in passes of a K-tile (a multiple
+// of 32, LG_TUNE_PPR_KTILE): a pass runs every iteration on its columns, so a
+// smaller tile re-reads the edge ids once more per pass but keeps the gathered
+// rows of a pass narrower.  The slots per warp range are LG_TUNE_PPR_RANGE.  Every snapshot's iterations are captured into one CUDA graph
 // and launched once.
 #include "lg_device.cuh"
 #include "lg_expand.cuh"
+#include "lg_tune.h"
 
 #include <algorithm>
 #include <vector>
 
 namespace lg {
 
-constexpr uint32_t kPprRange = 2048;
 constexpr int kPprThreads = 256;
 constexpr uint32_t kNoSeed = 0xffffffffu;
 
@@ -42,7 +45,9 @@ struct PprArgs {
 	uint32_t n_seeds;
 	double* carry_first;      // nranges x K
 	double* carry_last;       // nranges x K
-	uint32_t K;
+	uint32_t K;               // row length of y / x / carries
+	uint32_t col0;            // first column of this pass (a K-tile of CPL * 32 columns)
+	uint32_t range;           // virtual slots per warp range
 };
 
 template <int CPL>
@@ -52,7 +57,7 @@ __device__ __forceinline__ void ppr_finish(const PprArgs& a, uint32_t v, const d
 	const uint32_t sf = __ldg(a.seed_first + v);
 #pragma unroll
 	for (int i = 0; i < CPL; i++) {
-		const uint32_t c = lane + 32 * i;
+		const uint32_t c = a.col0 + lane + 32 * i;
 		double t = 0.0;
 		if (sf != kNoSeed)
 			for (uint32_t q = sf; q < a.n_seeds && a.seed_col[q].x == v; q++)
@@ -71,8 +76,8 @@ ppr_step(PprArgs a) {
 	if (r64 >= a.nranges) return;
 	const uint32_t r = (uint32_t)r64;
 	const bool last_range = r == a.nranges - 1;
-	const uint32_t ra = r * kPprRange;
-	const uint32_t rb = last_range ? a.total : min(a.total, ra + kPprRange);
+	const uint32_t ra = r * a.range;
+	const uint32_t rb = last_range ? a.total : min(a.total, ra + a.range);
 	uint32_t e_begin, e_end;
 	range_entries(a.pos, (uint32_t)a.in.V, ra, rb, last_range, &e_begin, &e_end);
 	const LevelTab* lt = a.in.lt;
@@ -89,10 +94,10 @@ ppr_step(PprArgs a) {
 			const uint32_t v = __shfl_sync(0xffffffffu, w.v, o);
 			if (st < ra) {
 #pragma unroll
-				for (int i = 0; i < CPL; i++) a.carry_first[(uint64_t)r * a.K + lane + 32 * i] = acc[i];
+				for (int i = 0; i < CPL; i++) a.carry_first[(uint64_t)r * a.K + a.col0 + lane + 32 * i] = acc[i];
 			} else if (en > rb) {
 #pragma unroll
-				for (int i = 0; i < CPL; i++) a.carry_last[(uint64_t)r * a.K + lane + 32 * i] = acc[i];
+				for (int i = 0; i < CPL; i++) a.carry_last[(uint64_t)r * a.K + a.col0 + lane + 32 * i] = acc[i];
 			} else {
 				ppr_finish<CPL>(a, v, acc);
 			}
@@ -120,7 +125,7 @@ ppr_step(PprArgs a) {
 					cur = o;
 				}
 				if (live) {
-					const double* row = a.y + (uint64_t)src * a.K;
+					const double* row = a.y + (uint64_t)src * a.K + a.col0;
 #pragma unroll
 					for (int i = 0; i < CPL; i++) acc[i] += __ldg(row + lane + 32 * i);
 				}
@@ -141,13 +146,13 @@ ppr_step(PprArgs a) {
 }
 
 // One warp per range boundary: the vertex that starts in range q-1 and
-// crosses q * kPprRange sums its carried rows in range order.
+// crosses q * range sums its carried rows in range order.
 template <int CPL>
 __global__ void ppr_fixup(PprArgs a) {
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint64_t q = (uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5) + 1;
 	if (q >= a.nranges) return;
-	const uint32_t s = (uint32_t)q * kPprRange;
+	const uint32_t s = (uint32_t)q * a.range;
 	uint32_t lo = 0, hi = (uint32_t)a.in.V;
 	while (lo < hi) {
 		const uint32_t mid = (lo + hi + 1) >> 1;
@@ -156,14 +161,15 @@ __global__ void ppr_fixup(PprArgs a) {
 	const uint32_t e = lo;
 	if (e >= a.in.V) return;
 	const uint32_t start = __ldg(a.pos + e), end = __ldg(a.pos + e + 1);
-	if (!(start < s && start >= s - kPprRange && end > s)) return;
-	const uint32_t r2 = (end - 1) / kPprRange;
+	if (!(start < s && start >= s - a.range && end > s)) return;
+	const uint32_t r2 = (end - 1) / a.range;
+	const uint32_t c0 = a.col0 + lane;
 	double t[CPL];
 #pragma unroll
-	for (int i = 0; i < CPL; i++) t[i] = __ldcg(a.carry_last + (uint64_t)(q - 1) * a.K + lane + 32 * i);
+	for (int i = 0; i < CPL; i++) t[i] = __ldcg(a.carry_last + (uint64_t)(q - 1) * a.K + c0 + 32 * i);
 	for (uint32_t x = (uint32_t)q; x <= r2; x++)
 #pragma unroll
-		for (int i = 0; i < CPL; i++) t[i] += __ldcg(a.carry_first + (uint64_t)x * a.K + lane + 32 * i);
+		for (int i = 0; i < CPL; i++) t[i] += __ldcg(a.carry_first + (uint64_t)x * a.K + c0 + 32 * i);
 	ppr_finish<CPL>(a, e, t);
 }
 
@@ -226,9 +232,15 @@ extern "C" lg_status lg_ppr(lg_snapshot* const* snaps, int n_snaps, const int64_
 	LG_TRY(yb[1].reserve(V * row));
 	LG_TRY(seedb.reserve(K * sizeof(uint2)));
 	LG_TRY(firstb.reserve(V * 4));
+	// launch parameters: columns per pass (a multiple of 32 dividing K) and
+	// slots per warp range
+	int ktile = (int)tune_value(s->device, LG_TUNE_PPR_KTILE);
+	ktile = std::min(K, std::max(32, ktile - ktile % 32));
+	while (K % ktile) ktile -= 32;
+	const uint32_t range = (uint32_t)tune_value(s->device, LG_TUNE_PPR_RANGE);
 	uint32_t maxr = 1;
 	for (int i = 0; i < n_snaps; i++)
-		maxr = std::max<uint32_t>(maxr, (uint32_t)((snaps[i]->in.n_frag_slots + kPprRange - 1) / kPprRange));
+		maxr = std::max<uint32_t>(maxr, (uint32_t)((snaps[i]->in.n_frag_slots + range - 1) / range));
 	LG_TRY(carry.reserve(2ull * maxr * row));
 	const bool dev_out = is_device_pointer(out);
 	double* res = out;
@@ -246,13 +258,16 @@ extern "C" lg_status lg_ppr(lg_snapshot* const* snaps, int n_snaps, const int64_
 	cudaGraphExec_t exec = nullptr;
 	LG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture");
 	uint64_t launches = 0;
+	cudaError_t cap = cudaSuccess;     // first error while capturing; the capture
+	                                   // is ended on every path below
 	for (int i = 0; i < n_snaps; i++) {
 		lg_snapshot* sn = snaps[i];
 		PprArgs a;
 		a.in = sn->view(1);
 		a.pos = sn->in.slot_off.as<uint32_t>();
 		a.total = (uint32_t)sn->in.n_frag_slots;
-		a.nranges = (uint32_t)std::max<uint64_t>(1, (a.total + kPprRange - 1) / kPprRange);
+		a.range = range;
+		a.nranges = (uint32_t)std::max<uint64_t>(1, (a.total + range - 1) / range);
 		a.outdeg = sn->out.deg.as<uint32_t>();
 		a.d = damping;
 		a.tele = 1.0 - damping;
@@ -263,34 +278,42 @@ extern "C" lg_status lg_ppr(lg_snapshot* const* snaps, int n_snaps, const int64_
 		a.carry_last = carry.as<double>() + (uint64_t)a.nranges * K;
 		a.K = (uint32_t)K;
 		double* xo = res + (uint64_t)i * V * K;
-		cudaMemsetAsync(yb[0].p, 0, V * row, st);
+		if (cap == cudaSuccess) cap = cudaMemsetAsync(yb[0].p, 0, V * row, st);
 		ppr_seed_init<<<grid_for(K, 256), 256, 0, st>>>(seedb.as<uint2>(), K, a.outdeg, K,
 				yb[0].as<double>());
 		launches++;
 		if (iterations == 0) {
-			cudaMemsetAsync(xo, 0, V * row, st);
+			if (cap == cudaSuccess) cap = cudaMemsetAsync(xo, 0, V * row, st);
 			ppr_seed_x<<<grid_for(K, 256), 256, 0, st>>>(seedb.as<uint2>(), K, K, xo);
 			launches++;
 		}
-		for (int it = 0; it < iterations; it++) {
-			a.y = yb[it & 1].as<double>();
-			a.y_next = yb[(it + 1) & 1].as<double>();
-			a.x_out = (it == iterations - 1) ? xo : nullptr;
-			switch (K / 32) {
-			case 1: launch_ppr_iteration<1>(a, st); break;
-			case 2: launch_ppr_iteration<2>(a, st); break;
-			case 3: launch_ppr_iteration<3>(a, st); break;
-			case 4: launch_ppr_iteration<4>(a, st); break;
-			case 5: launch_ppr_iteration<5>(a, st); break;
-			case 6: launch_ppr_iteration<6>(a, st); break;
-			case 7: launch_ppr_iteration<7>(a, st); break;
-			default: launch_ppr_iteration<8>(a, st); break;
+		// column tiles are independent: each runs all iterations on its columns
+		for (int c0 = 0; c0 < K; c0 += ktile) {
+			a.col0 = (uint32_t)c0;
+			for (int it = 0; it < iterations; it++) {
+				a.y = yb[it & 1].as<double>();
+				a.y_next = yb[(it + 1) & 1].as<double>();
+				a.x_out = (it == iterations - 1) ? xo : nullptr;
+				switch (ktile / 32) {
+				case 1: launch_ppr_iteration<1>(a, st); break;
+				case 2: launch_ppr_iteration<2>(a, st); break;
+				case 3: launch_ppr_iteration<3>(a, st); break;
+				case 4: launch_ppr_iteration<4>(a, st); break;
+				case 5: launch_ppr_iteration<5>(a, st); break;
+				case 6: launch_ppr_iteration<6>(a, st); break;
+				case 7: launch_ppr_iteration<7>(a, st); break;
+				default: launch_ppr_iteration<8>(a, st); break;
+				}
+				launches += a.nranges > 1 ? 2 : 1;
 			}
-			launches += a.nranges > 1 ? 2 : 1;
 		}
 	}
+	if (cap == cudaSuccess) cap = cudaGetLastError();
 	cudaError_t ce = cudaStreamEndCapture(st, &graph);
-	if (ce != cudaSuccess) return cuda_status(ce, "graph capture");
+	if (cap != cudaSuccess || ce != cudaSuccess) {
+		if (graph) cudaGraphDestroy(graph);
+		return cuda_status(cap != cudaSuccess ? cap : ce, "graph capture");
+	}
 	ce = cudaGraphInstantiate(&exec, graph, 0);
 	if (ce != cudaSuccess) { cudaGraphDestroy(graph); return cuda_status(ce, "graph instantiate"); }
 	ce = cudaGraphLaunch(exec, st);

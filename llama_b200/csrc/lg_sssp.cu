@@ -17,12 +17,13 @@
 // and weights in one array each, no deletion bits) instead of the levels.
 #include "lg_expand.cuh"
 #include "lg_flat.cuh"
+#include "lg_tune.h"
 
 namespace lg {
 
 constexpr uint32_t kInf = LG_UNREACHED;
 constexpr int kSsspThreads = 256;
-constexpr uint32_t kSsspRange = 1024;     // slots per warp range
+// slots per warp range: LG_TUNE_SSSP_RANGE (1024 by default)
 
 __global__ void sssp_init(uint32_t* dist, uint32_t* stamp, uint32_t* fstamp,
 		uint64_t V, uint32_t root, uint32_t* queue) {
@@ -66,24 +67,25 @@ __device__ __forceinline__ void wq_add(bool take, uint32_t item, uint32_t* sbuf,
 
 // One relaxation round over the near queue.  The queue's slot space
 // (pos = exclusive prefix of the queued vertices' slot counts, pos[qlen] the
-// total, both written earlier on the stream) is cut into kSsspRange-slot
+// total, both written earlier on the stream) is cut into `range`-slot
 // ranges that the grid's warps take in turn, so a hub in the queue is spread
 // over many warps.  ctr[0] near-next length, ctr[1] far length (starts at
 // the current pile size), ctr[2] relaxations.
 __global__ void __launch_bounds__(kSsspThreads)
 sssp_relax(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
 		uint32_t* dist, uint32_t* stamp, uint32_t* fstamp, uint32_t round, uint32_t epoch,
-		uint32_t hi, uint32_t* near_next, uint32_t* far, unsigned long long* ctr) {
+		uint32_t hi, uint32_t* near_next, uint32_t* far, unsigned long long* ctr,
+		uint32_t range) {
 	__shared__ uint32_t sbuf[kSsspThreads / 32][2][kPushBuf];
 	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
 	const uint32_t total = __ldg(pos + qlen);
-	const uint32_t nranges = (total + kSsspRange - 1) / kSsspRange;
+	const uint32_t nranges = (total + range - 1) / range;
 	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
 	unsigned long long relax = 0;
 	uint32_t nn = 0, nf = 0;       // staged near / far appends of this warp
 	for (uint32_t r = warp; r < nranges; r += nwarps) {
-		range_for_each(out, queue, pos, qlen, total, nranges, kSsspRange, r,
+		range_for_each(out, queue, pos, qlen, total, nranges, range, r,
 			[&](bool act, uint32_t, uint32_t ov, uint32_t nbr, uint32_t lv, uint32_t idx) {
 				bool to_near = false, to_far = false;
 				if (act) {
@@ -191,6 +193,7 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 	int sms = 148;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
 	const unsigned relax_blocks = (unsigned)sms * 8u;   // persistent over the ranges
+	const uint32_t range = (uint32_t)tune_value(s->device, LG_TUNE_SSSP_RANGE);
 	const bool dev_out = is_device_pointer(dist);
 	uint32_t* d = dist;
 	if (!dev_out) { LG_TRY(sc[4].reserve(V * 4)); d = sc[4].as<uint32_t>(); }
@@ -254,7 +257,7 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 		list_slots<<<grid_for(qlen, 256), 256, 0, st>>>(out, q, (uint32_t)qlen, qcnt);
 		LG_TRY(exclusive_scan_u32(qcnt, qpos, qlen, sc[8], st, nullptr));
 		sssp_relax<<<relax_blocks, kSsspThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, d,
-				stamp, fstamp, round, epoch, hi, qn, far, ctr);
+				stamp, fstamp, round, epoch, hi, qn, far, ctr, range);
 		LG_CUDA(cudaGetLastError(), "sssp_relax");
 		s->launches += 5;
 		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");

@@ -18,6 +18,10 @@ struct Limits { int64_t lo, hi, def; };
 // workloads; lo/hi bound what a kernel accepts
 const Limits kLimits[LG_TUNE_COUNT] = {
 	{0, 32, 0},         // LG_TUNE_PR_CTAS_PER_SM
+	{32, 256, 256},     // LG_TUNE_PPR_KTILE (rounded down to a multiple of 32 dividing K)
+	{256, 16384, 2048}, // LG_TUNE_PPR_RANGE
+	{256, 16384, 1024}, // LG_TUNE_SSSP_RANGE
+	{32, 1u << 20, 512},// LG_TUNE_MS_HEAVY
 };
 
 std::mutex g_mu;

@@ -265,7 +265,11 @@ class Tape:
     __del__ = close
 
 
-TUNABLES = {"pr_ctas_per_sm": _lib.LG_TUNE_PR_CTAS_PER_SM}
+TUNABLES = {"pr_ctas_per_sm": _lib.LG_TUNE_PR_CTAS_PER_SM,
+            "ppr_ktile": _lib.LG_TUNE_PPR_KTILE,
+            "ppr_range": _lib.LG_TUNE_PPR_RANGE,
+            "sssp_range": _lib.LG_TUNE_SSSP_RANGE,
+            "ms_heavy": _lib.LG_TUNE_MS_HEAVY}
 
 
 def tune_set(device, name, value):
@@ -421,6 +425,26 @@ class Snapshot:
         fn = lib.lg_bc_batched if batched else lib.lg_bc
         check(fn(self._h, ptr(src), len(src), ptr(res)))
         return res
+
+    def autotune(self, names=None):
+        """Measure the launch parameters `names` (TUNABLES keys, default all)
+        on this snapshot and keep the fastest (``lg_autotune``); returns
+        {name: {"chosen": value, "ms": {value: median ms}}}."""
+        names = list(TUNABLES) if names is None else list(names)
+        mask = 0
+        for n in names:
+            mask |= 1 << TUNABLES[n]
+        trials = (_lib.lg_tune_trial * 64)()
+        count = C.c_int()
+        check(lib.lg_autotune(self._h, mask, trials, 64, C.byref(count)))
+        by_key = {v: k for k, v in TUNABLES.items()}
+        out = {}
+        for t in trials[:count.value]:
+            d = out.setdefault(by_key[t.key], {"chosen": None, "ms": {}})
+            d["ms"][int(t.value)] = t.ms
+            if t.chosen:
+                d["chosen"] = int(t.value)
+        return out
 
     def pagerank_fwd(self, weights, teleport, damping=0.85, tol=1e-12, max_iter=10000,
                      keep_tape=True, out=None):
