@@ -452,6 +452,13 @@ def run_lg(args):
     launch_s = statistics.median(diffs) / 1e3
     peak, peak_kind = measured_peak()
     achieved = pr_bytes / launch_s / 1e9
+    # the floor of a kernel that gathers one 8-byte value per edge: the
+    # PageRank iteration's loads alone (lg_pagerank_gather_pass) over the same
+    # flat in-CSR, median of 5 timed passes after a warm-up
+    sn.flatten(1)
+    sn.gather_pass_async()
+    floor_ms = statistics.median(_timed(stream, sn.gather_pass_async)[1] for _ in range(5))
+    sn.unflatten()
     roofline = {"bound": "hbm", "kernel": "pr_flat_step", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
@@ -466,6 +473,13 @@ def run_lg(args):
                 "launch_ms_source": "CUDA events on the store's stream: "
                                     "(t(2k iterations) - t(k iterations)) / k, median of 3",
                 "pr_call_ms": pr_ms / args.steps,
+                "gather_floor": {
+                    "ms": floor_ms, "launch_over_floor": launch_s * 1e3 / floor_ms,
+                    "frac_at_floor": pr_bytes / (floor_ms / 1e3) / 1e9 / peak,
+                    "what": "lg_pagerank_gather_pass: the iteration's id loads and one 8-byte "
+                            "gather per edge in the same lane layout, without the row sums; "
+                            "frac_at_floor is the survey-model fraction a kernel running at "
+                            "this floor would reach"},
                 "traffic": args.traffic,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                   "full-size launch, passed with --traffic"

@@ -95,10 +95,10 @@ extern "C" lg_status lg_autotune(lg_snapshot* sn, unsigned keys, lg_tune_trial* 
 			[=]() { return lg_pagerank_pull(sn, 6, 0.85, dout); }});
 	if ((keys & (1u << LG_TUNE_PPR_KTILE)) && want_ppr)
 		probes.push_back({LG_TUNE_PPR_KTILE, {32, 64, 128, 256},
-			[=, &seeds]() { return lg_ppr(one, 1, seeds.data(), 256, 2, 0.85, dout); }});
+			[=, &seeds]() { return lg_ppr(one, 1, seeds.data(), 256, 4, 0.85, dout); }});
 	if ((keys & (1u << LG_TUNE_PPR_RANGE)) && want_ppr)
 		probes.push_back({LG_TUNE_PPR_RANGE, {1024, 2048, 4096},
-			[=, &seeds]() { return lg_ppr(one, 1, seeds.data(), 256, 2, 0.85, dout); }});
+			[=, &seeds]() { return lg_ppr(one, 1, seeds.data(), 256, 4, 0.85, dout); }});
 	if ((keys & (1u << LG_TUNE_SSSP_RANGE)) && weighted)
 		probes.push_back({LG_TUNE_SSSP_RANGE, {512, 1024, 2048, 4096},
 			[=, &roots]() {

@@ -375,11 +375,15 @@ __global__ void ms_reach(const int32_t* levels, const uint32_t* outdeg, uint64_t
 // FP64 here.  A pass serves 64 sources: the BFS levels are the multi-source
 // BFS above (lk[v] = the sources that have v at depth k, kept for every
 // depth), and sigma / delta are 64 doubles per vertex.  An edge v->w is a
-// down edge for exactly the sources in lk[v] & lk+1[w], so a sweep over the
-// out-edges of a level reads one 8-byte mask per edge and touches sigma and
-// delta only for those sources: the work follows the (source, down edge)
-// pairs, not 64 x every edge.  Sums use FP64 atomics, so results agree with
-// an exact evaluation to ~1e-15 relative, not bit for bit.
+// down edge for exactly the sources in lk[v] & lk+1[w], so a sweep reads one
+// 8-byte mask per edge and touches sigma and delta only for those sources:
+// the work follows the (source, down edge) pairs, not 64 x every edge.  Both
+// sweeps pull: sigma of level k + 1 over its vertices' in-edges, delta of
+// level k over its vertices' out-edges, each vertex's sums kept in registers
+// along its run of edges and added once per run (FP64 atomics only where a
+// run is split between warps), so results agree with an exact evaluation to
+// ~1e-15 relative, not bit for bit.  Without an in-CSR the sigma sweep
+// pushes along out-edges instead, one atomic per (edge, source) pair.
 // ---------------------------------------------------------------------------
 
 // Sources of a pass: level-0 masks, sigma = 1, the sources' own-lane mask.
@@ -399,8 +403,10 @@ __global__ void bcm_roots(const int64_t* src, int n, u64* seen, u64* l0, u64* ow
 }
 
 // sigma[w][j] += sigma[v][j] over the out-edges v->w of level k's vertices
-// for the sources j in lk[v] & lk1[w]; the warp takes such edges one at a
-// time, lane j serving sources j and j + 32.
+// for the sources j in lk[v] & lk1[w]; the warp takes such edges kMsBatch at
+// a time (their sigma rows are loaded before any add, so the loads of the
+// batch overlap), lane j serving sources j and j + 32.
+constexpr int kMsBatch = 4;
 __global__ void __launch_bounds__(kMsThreads)
 bcm_sigma(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
 		const u64* lk, const u64* lk1, double* sigma) {
@@ -416,18 +422,102 @@ bcm_sigma(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen
 				const u64 m = act ? (__ldg(lk + v) & __ldg(lk1 + w)) : 0ull;
 				unsigned todo = __ballot_sync(0xffffffffu, m != 0);
 				while (todo) {
-					const int t = __ffs(todo) - 1;
-					todo &= todo - 1;
-					const uint32_t tv = __shfl_sync(0xffffffffu, v, t);
-					const uint32_t tw = __shfl_sync(0xffffffffu, w, t);
-					const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)m, t);
-					const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(m >> 32), t);
-					const double* sv = sigma + (uint64_t)tv * kMsMaxRoots;
-					double* sw = sigma + (uint64_t)tw * kMsMaxRoots;
-					if ((lo >> lane) & 1u) atomicAdd(sw + lane, __ldcg(sv + lane));
-					if ((hi >> lane) & 1u) atomicAdd(sw + 32 + lane, __ldcg(sv + 32 + lane));
+					uint32_t tw[kMsBatch];
+					bool b0[kMsBatch], b1[kMsBatch];
+					double x0[kMsBatch], x1[kMsBatch];
+#pragma unroll
+					for (int u = 0; u < kMsBatch; u++) {
+						const int t = todo ? __ffs(todo) - 1 : -1;   // warp-uniform
+						todo &= todo - 1;
+						tw[u] = 0;
+						b0[u] = b1[u] = false;
+						x0[u] = x1[u] = 0.0;
+						if (t >= 0) {
+							const uint32_t tv = __shfl_sync(0xffffffffu, v, t);
+							tw[u] = __shfl_sync(0xffffffffu, w, t);
+							const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)m, t);
+							const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(m >> 32), t);
+							const double* sv = sigma + (uint64_t)tv * kMsMaxRoots;
+							b0[u] = (lo >> lane) & 1u;
+							b1[u] = (hi >> lane) & 1u;
+							if (b0[u]) x0[u] = __ldcg(sv + lane);
+							if (b1[u]) x1[u] = __ldcg(sv + 32 + lane);
+						}
+					}
+#pragma unroll
+					for (int u = 0; u < kMsBatch; u++) {
+						double* sw = sigma + (uint64_t)tw[u] * kMsMaxRoots;
+						if (b0[u]) atomicAdd(sw + lane, x0[u]);
+						if (b1[u]) atomicAdd(sw + 32 + lane, x1[u]);
+					}
 				}
 			});
+	}
+}
+
+// The same sums pulled: for the vertices w of level k + 1's queue, over their
+// in-edges v -> w (in-CSR ranges grouped by w), sigma[w][j] += sigma[v][j]
+// for the sources j in lk[v] & lk1[w].  Each lane keeps w's two partial sums
+// in registers over the run of w's in-edges and adds them to sigma[w] once
+// per run, instead of one atomic per (edge, source) pair; kMsBatch edges'
+// row loads are issued before their sums.
+__global__ void __launch_bounds__(kMsThreads)
+bcm_sigma_pull(SnapCsr in, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
+		const u64* lk, const u64* lk1, double* sigma) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t total = __ldg(pos + qlen);
+	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	const uint32_t range = ms_range(total, nwarps);
+	const uint32_t nranges = (total + range - 1) / range;
+	for (uint32_t r = warp; r < nranges; r += nwarps) {
+		uint32_t cur = 0xffffffffu;
+		double a0 = 0.0, a1 = 0.0;
+		range_for_each(in, queue, pos, qlen, total, nranges, range, r,
+			[&](bool act, uint32_t, uint32_t w, uint32_t v, uint32_t, uint32_t) {
+				const u64 m = act ? (__ldg(lk + v) & __ldg(lk1 + w)) : 0ull;
+				unsigned todo = __ballot_sync(0xffffffffu, m != 0);
+				while (todo) {
+					uint32_t tw[kMsBatch];
+					double p0[kMsBatch], p1[kMsBatch];
+#pragma unroll
+					for (int u = 0; u < kMsBatch; u++) {
+						const int t = todo ? __ffs(todo) - 1 : -1;   // warp-uniform
+						todo &= todo - 1;
+						tw[u] = 0xffffffffu;
+						p0[u] = p1[u] = 0.0;
+						if (t >= 0) {
+							tw[u] = __shfl_sync(0xffffffffu, w, t);
+							const uint32_t tv = __shfl_sync(0xffffffffu, v, t);
+							const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)m, t);
+							const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(m >> 32), t);
+							const double* sv = sigma + (uint64_t)tv * kMsMaxRoots;
+							if ((lo >> lane) & 1u) p0[u] = __ldcg(sv + lane);
+							if ((hi >> lane) & 1u) p1[u] = __ldcg(sv + 32 + lane);
+						}
+					}
+#pragma unroll
+					for (int u = 0; u < kMsBatch; u++) {
+						if (tw[u] == 0xffffffffu) continue;          // warp-uniform
+						if (tw[u] != cur) {
+							if (cur != 0xffffffffu) {
+								double* sw = sigma + (uint64_t)cur * kMsMaxRoots;
+								if (a0 != 0.0) atomicAdd(sw + lane, a0);
+								if (a1 != 0.0) atomicAdd(sw + 32 + lane, a1);
+							}
+							cur = tw[u];
+							a0 = a1 = 0.0;
+						}
+						a0 += p0[u];
+						a1 += p1[u];
+					}
+				}
+			});
+		if (cur != 0xffffffffu) {
+			double* sw = sigma + (uint64_t)cur * kMsMaxRoots;
+			if (a0 != 0.0) atomicAdd(sw + lane, a0);
+			if (a1 != 0.0) atomicAdd(sw + 32 + lane, a1);
+		}
 	}
 }
 
@@ -454,25 +544,43 @@ bcm_delta(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen
 				const u64 m = act ? (__ldg(lk + v) & __ldg(lk1 + w)) : 0ull;
 				unsigned todo = __ballot_sync(0xffffffffu, m != 0);
 				while (todo) {
-					const int t = __ffs(todo) - 1;
-					todo &= todo - 1;
-					const uint32_t tv = __shfl_sync(0xffffffffu, v, t);
-					const uint32_t tw = __shfl_sync(0xffffffffu, w, t);
-					const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)m, t);
-					const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(m >> 32), t);
-					if (tv != cur) {
-						if (cur != 0xffffffffu) {
-							double* dv = delta + (uint64_t)cur * kMsMaxRoots;
-							if (a0 != 0.0) atomicAdd(dv + lane, a0);
-							if (a1 != 0.0) atomicAdd(dv + 32 + lane, a1);
+					// kMsBatch edges: all their row loads first, then the sums
+					// in edge order
+					uint32_t tv[kMsBatch];
+					double p0[kMsBatch], p1[kMsBatch];
+#pragma unroll
+					for (int u = 0; u < kMsBatch; u++) {
+						const int t = todo ? __ffs(todo) - 1 : -1;   // warp-uniform
+						todo &= todo - 1;
+						tv[u] = 0xffffffffu;
+						p0[u] = p1[u] = 0.0;
+						if (t >= 0) {
+							tv[u] = __shfl_sync(0xffffffffu, v, t);
+							const uint32_t tw = __shfl_sync(0xffffffffu, w, t);
+							const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)m, t);
+							const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(m >> 32), t);
+							const double* sv = sigma + (uint64_t)tv[u] * kMsMaxRoots;
+							const double* qw = sigma + (uint64_t)tw * kMsMaxRoots;
+							if ((lo >> lane) & 1u) p0[u] = __ldg(sv + lane) * __ldg(qw + lane);
+							if ((hi >> lane) & 1u)
+								p1[u] = __ldg(sv + 32 + lane) * __ldg(qw + 32 + lane);
 						}
-						cur = tv;
-						a0 = a1 = 0.0;
 					}
-					const double* sv = sigma + (uint64_t)tv * kMsMaxRoots;
-					const double* qw = sigma + (uint64_t)tw * kMsMaxRoots;
-					if ((lo >> lane) & 1u) a0 += __ldg(sv + lane) * __ldg(qw + lane);
-					if ((hi >> lane) & 1u) a1 += __ldg(sv + 32 + lane) * __ldg(qw + 32 + lane);
+#pragma unroll
+					for (int u = 0; u < kMsBatch; u++) {
+						if (tv[u] == 0xffffffffu) continue;          // warp-uniform
+						if (tv[u] != cur) {
+							if (cur != 0xffffffffu) {
+								double* dv = delta + (uint64_t)cur * kMsMaxRoots;
+								if (a0 != 0.0) atomicAdd(dv + lane, a0);
+								if (a1 != 0.0) atomicAdd(dv + 32 + lane, a1);
+							}
+							cur = tv[u];
+							a0 = a1 = 0.0;
+						}
+						a0 += p0[u];
+						a1 += p1[u];
+					}
 				}
 			});
 		if (cur != 0xffffffffu) {
@@ -673,12 +781,25 @@ extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int 
 						seen, lk1, nullptr, outdeg, q2, ctr);
 				s->launches += 5;
 			}
-			bcm_sigma<<<grid, kMsThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, lk, lk1, sigma);
+			if (!has_in) {
+				// push along the level's out-edges (one atomic per down pair)
+				bcm_sigma<<<grid, kMsThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, lk, lk1,
+						sigma);
+				s->launches++;
+			}
 			LG_CUDA(cudaGetLastError(), "bc batched forward");
-			s->launches++;
 			LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
 			LG_CUDA(cudaStreamSynchronize(st), "bc batched");
 			s->d2h_bytes += sizeof(h) + sizeof(unsigned long long);
+			if (has_in && h[0] > 0) {
+				// pull into the new level over its in-edges
+				list_slots<<<grid_for(h[0], B), B, 0, st>>>(in, q2, (uint32_t)h[0], qcnt);
+				LG_TRY(exclusive_scan_u32(qcnt, qpos, h[0], sc[9], st, nullptr));
+				bcm_sigma_pull<<<grid, kMsThreads, 0, st>>>(in, q2, qpos, (uint32_t)h[0], lk, lk1,
+						sigma);
+				LG_CUDA(cudaGetLastError(), "bc batched sigma");
+				s->launches += 5;
+			}
 			qoff.push_back(qoff[k + 1] + h[0]);
 			mf = h[1];
 			mu -= std::min(mu, (uint64_t)mf);

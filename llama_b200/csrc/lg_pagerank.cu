@@ -25,8 +25,9 @@
 // and joins the lanes with one segmented warp scan keyed by the head bits; a
 // vertex that runs past a tile boundary leaves partials (carry_first,
 // carry_last) that pr_flat_fixup adds.  No block barriers: each warp stages
-// its finished row sums in its own shared memory.  Vertices without in-edges have the constant rank (1-d)/N after the first
-// iteration and are written once (pr_empty_rows).
+// its finished row sums in its own shared memory.  Vertices without
+// in-edges have the constant rank (1-d)/N after the first iteration and are
+// written once (pr_empty_rows).
 //
 // lg_pagerank_pull_noalloc cannot hold the E-sized flat array, so it walks
 // the fragments directly every iteration (pr_pull_step, one CTA per 1024
@@ -344,6 +345,95 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 	if (!dev_out) {
 		LG_TRY(copy_out(s, ranks, pr_buf, V * sizeof(double)));
 		LG_CUDA(cudaStreamSynchronize(st), "pagerank");
+	}
+	return LG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The gather floor: pr_flat_step's loads without its sums.
+// ---------------------------------------------------------------------------
+
+namespace lg {
+
+// Lane j of the warp owning tile t loads the ids of edges e0 + 8j .. + 7
+// (one 32-byte load, evict-first, as pr_flat_step) and gathers x at them;
+// the warp's total goes to out[t].
+__global__ void __launch_bounds__(kFlatWarps * 32)
+pr_gather_floor(const uint32_t* ids, uint32_t E, uint32_t ntiles, const double* x,
+		double* out) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t t = blockIdx.x * kFlatWarps + (threadIdx.x >> 5);
+	if (t >= ntiles) return;
+	const uint32_t eb = t * kFlatTile + lane * kFlatPerLane;
+	uint32_t id[kFlatPerLane];
+	if (eb + kFlatPerLane <= E) {
+		asm("ld.global.cs.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+			: "=r"(id[0]), "=r"(id[1]), "=r"(id[2]), "=r"(id[3]),
+			  "=r"(id[4]), "=r"(id[5]), "=r"(id[6]), "=r"(id[7])
+			: "l"(ids + eb));
+	} else {
+#pragma unroll
+		for (int i = 0; i < kFlatPerLane; i++) id[i] = eb + i < E ? __ldcs(ids + eb + i) : kNoId;
+	}
+	double v[kFlatPerLane];
+#pragma unroll
+	for (int i = 0; i < kFlatPerLane; i++) v[i] = id[i] != kNoId ? __ldg(x + id[i]) : 0.0;
+	double s = 0.0;
+#pragma unroll
+	for (int i = 0; i < kFlatPerLane; i++) s += v[i];
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+	if (lane == 0) out[t] = s;
+}
+
+__global__ void sum_doubles(const double* a, uint32_t n, double* out) {
+	double s = 0.0;
+	for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) s += a[i];
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+	__shared__ double w[32];
+	if ((threadIdx.x & 31u) == 0) w[threadIdx.x >> 5] = s;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (uint32_t i = 0; i < blockDim.x / 32; i++) t += w[i];
+		*out = t;
+	}
+}
+
+} // namespace lg
+
+extern "C" lg_status lg_pagerank_gather_pass(lg_snapshot* sn, double* checksum) {
+	clear_error();
+	if (!sn) return set_error(LG_EINVAL, "null snapshot");
+	FlatCsr* f = sn->flat[1];
+	if (!f) return set_error(LG_ESTATE, "flatten the in-CSR first (lg_snapshot_flatten)");
+	lg_store* s = sn->store;
+	LG_CUDA(cudaSetDevice(s->device), "cudaSetDevice");
+	cudaStream_t st = s->stream;
+	const uint64_t V = sn->V;
+	DevBuf* sc = s->scratch;
+	LG_TRY(sc[0].reserve(V * sizeof(double)));
+	LG_TRY(sc[2].reserve((std::max<uint32_t>(f->ntiles, 1) + 1) * sizeof(double)));
+	double* x = sc[0].as<double>();
+	double* part = sc[2].as<double>();
+	pr_init<<<grid_for(V, 256), 256, 0, st>>>(sn->out.deg.as<uint32_t>(), V, 1.0 / (double)V, x,
+			nullptr);
+	s->launches++;
+	if (f->ntiles > 0) {
+		pr_gather_floor<<<flat_sweep_blocks(f->ntiles), kFlatWarps * 32, 0, st>>>(
+				f->ids.as<uint32_t>(), (uint32_t)f->E, f->ntiles, x, part);
+		sum_doubles<<<1, 1024, 0, st>>>(part, f->ntiles, part + f->ntiles);
+		s->launches += 2;
+	} else {
+		LG_CUDA(cudaMemsetAsync(part, 0, sizeof(double), st), "memset");
+	}
+	LG_CUDA(cudaGetLastError(), "pr_gather_floor");
+	if (checksum) {
+		LG_CUDA(cudaMemcpyAsync(checksum, part + (f->ntiles > 0 ? f->ntiles : 0), sizeof(double),
+				cudaMemcpyDeviceToHost, st), "d2h");
+		LG_CUDA(cudaStreamSynchronize(st), "gather pass");
+		s->d2h_bytes += sizeof(double);
 	}
 	return LG_OK;
 }

@@ -227,7 +227,12 @@ extern "C" lg_status lg_ppr(lg_snapshot* const* snaps, int n_snaps, const int64_
 		if (k == 0 || sc[k].x != sc[k - 1].x) firsts.push_back({sc[k].x, (uint32_t)k});
 
 	const uint64_t row = (uint64_t)K * 8;
-	DevBuf yb[2], seedb, firstb, carry, resb;
+	// the store's scratch (kept for the next call, contents not preserved)
+	DevBuf* yb = s->scratch;         // scratch[0], [1]: the two V x K blocks
+	DevBuf& carry = s->scratch[2];
+	DevBuf& seedb = s->scratch[3];
+	DevBuf& firstb = s->scratch[4];
+	DevBuf& resb = s->scratch[5];
 	LG_TRY(yb[0].reserve(V * row));
 	LG_TRY(yb[1].reserve(V * row));
 	LG_TRY(seedb.reserve(K * sizeof(uint2)));

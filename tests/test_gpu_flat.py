@@ -134,3 +134,22 @@ def test_flatten_errors():
             assert sn.is_flat(0)
             lv, res = sn.bfs(0)                # top-down only, on the flat out-CSR
             assert lv[0] == 0
+
+
+def test_gather_pass_checksum_and_state():
+    """lg_pagerank_gather_pass gathers pr0 / out_degree(src) once per live
+    in-edge of the flat in-CSR; it needs the snapshot flattened."""
+    from llama_b200 import LgError
+    spec = workloads.rmat_multiversion(scale=12, seed=5, levels=3, level0=0.9, delete=0.02)
+    hg = HostGraph.from_spec(spec)
+    with Store() as st:
+        st.ingest(hg)
+        with st.snapshot() as sn:
+            with pytest.raises(LgError):
+                sn.gather_pass()
+            sn.flatten(1)
+            got = sn.gather_pass()
+            off, nb = sn.adjacency(1)
+            od = sn.out_degrees().astype(np.float64)
+            want = float(np.sum((1.0 / sn.max_nodes) / od[nb]))
+            assert abs(got - want) <= 1e-12 * abs(want)
