@@ -524,9 +524,21 @@ bcm_sigma_pull(SnapCsr in, const uint32_t* queue, const uint32_t* pos, uint32_t 
 // delta[v][j] = sum over down edges v->w (j in lk[v] & lk1[w]) of
 // sigma[v][j] * q[w][j], for level k's vertices, where q[w][j] =
 // (1 + delta[w][j]) / sigma[w][j] has already replaced sigma[w][j] for the
-// sources that have w at depth k + 1 (bcm_quot), so an edge costs a multiply,
-// not a division; edges come grouped by v, so each lane keeps v's two partial
-// sums and adds them to delta once per run of v.
+// sources that have w at depth k + 1 (bcm_quot), so an edge costs an add, not
+// a division: sigma[v][j] is the same for all of v's edges and multiplies
+// the sum of q once per run.  Edges come grouped by v; each lane keeps v's
+// two partial sums (sources j and j + 32) over the run and adds
+// sigma[v][j] * sum to delta once per run; the q loads of kMsBatch edges are
+// issued before their adds.
+__device__ __forceinline__ void bcm_delta_flush(uint32_t v, double a0, double a1,
+		const double* sigma, double* delta) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const double* sv = sigma + (uint64_t)v * kMsMaxRoots;
+	double* dv = delta + (uint64_t)v * kMsMaxRoots;
+	if (a0 != 0.0) atomicAdd(dv + lane, __ldg(sv + lane) * a0);
+	if (a1 != 0.0) atomicAdd(dv + 32 + lane, __ldg(sv + 32 + lane) * a1);
+}
+
 __global__ void __launch_bounds__(kMsThreads)
 bcm_delta(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
 		const u64* lk, const u64* lk1, const double* sigma, double* delta) {
@@ -544,8 +556,6 @@ bcm_delta(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen
 				const u64 m = act ? (__ldg(lk + v) & __ldg(lk1 + w)) : 0ull;
 				unsigned todo = __ballot_sync(0xffffffffu, m != 0);
 				while (todo) {
-					// kMsBatch edges: all their row loads first, then the sums
-					// in edge order
 					uint32_t tv[kMsBatch];
 					double p0[kMsBatch], p1[kMsBatch];
 #pragma unroll
@@ -559,22 +569,16 @@ bcm_delta(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen
 							const uint32_t tw = __shfl_sync(0xffffffffu, w, t);
 							const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)m, t);
 							const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(m >> 32), t);
-							const double* sv = sigma + (uint64_t)tv[u] * kMsMaxRoots;
 							const double* qw = sigma + (uint64_t)tw * kMsMaxRoots;
-							if ((lo >> lane) & 1u) p0[u] = __ldg(sv + lane) * __ldg(qw + lane);
-							if ((hi >> lane) & 1u)
-								p1[u] = __ldg(sv + 32 + lane) * __ldg(qw + 32 + lane);
+							if ((lo >> lane) & 1u) p0[u] = __ldg(qw + lane);
+							if ((hi >> lane) & 1u) p1[u] = __ldg(qw + 32 + lane);
 						}
 					}
 #pragma unroll
 					for (int u = 0; u < kMsBatch; u++) {
 						if (tv[u] == 0xffffffffu) continue;          // warp-uniform
 						if (tv[u] != cur) {
-							if (cur != 0xffffffffu) {
-								double* dv = delta + (uint64_t)cur * kMsMaxRoots;
-								if (a0 != 0.0) atomicAdd(dv + lane, a0);
-								if (a1 != 0.0) atomicAdd(dv + 32 + lane, a1);
-							}
+							if (cur != 0xffffffffu) bcm_delta_flush(cur, a0, a1, sigma, delta);
 							cur = tv[u];
 							a0 = a1 = 0.0;
 						}
@@ -583,11 +587,7 @@ bcm_delta(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen
 					}
 				}
 			});
-		if (cur != 0xffffffffu) {
-			double* dv = delta + (uint64_t)cur * kMsMaxRoots;
-			if (a0 != 0.0) atomicAdd(dv + lane, a0);
-			if (a1 != 0.0) atomicAdd(dv + 32 + lane, a1);
-		}
+		if (cur != 0xffffffffu) bcm_delta_flush(cur, a0, a1, sigma, delta);
 	}
 }
 
