@@ -454,10 +454,15 @@ def run_lg(args):
     achieved = pr_bytes / launch_s / 1e9
     # the floor of a kernel that gathers one 8-byte value per edge: the
     # PageRank iteration's loads alone (lg_pagerank_gather_pass) over the same
-    # flat in-CSR, median of 5 timed passes after a warm-up
+    # flat in-CSR, per pass as (t(2k passes) - t(k passes)) / k, median of 3
     sn.flatten(1)
-    sn.gather_pass_async()
-    floor_ms = statistics.median(_timed(stream, sn.gather_pass_async)[1] for _ in range(5))
+    sn.gather_pass_async(k)
+    fd = []
+    for _ in range(3):
+        _, t1 = _timed(stream, lambda: sn.gather_pass_async(k))
+        _, t2 = _timed(stream, lambda: sn.gather_pass_async(2 * k))
+        fd.append((t2 - t1) / k)
+    floor_ms = statistics.median(fd)
     sn.unflatten()
     roofline = {"bound": "hbm", "kernel": "pr_flat_step", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -358,16 +358,17 @@ lg_status lg_pagerank_push(lg_snapshot* snap, int iterations, double damping,
 lg_status lg_pagerank_pull_noalloc(lg_snapshot* snap, int iterations,
 		double damping, double* ranks);
 
-/* Diagnostic (no reference counterpart): one pass of the PageRank iteration's
- * memory traffic alone over the snapshot's flat in-CSR (lg_snapshot_flatten
+/* Diagnostic (no reference counterpart): `passes` passes of the PageRank
+ * iteration's memory traffic alone over the snapshot's flat in-CSR (lg_snapshot_flatten
  * direction 1 first, else LG_ESTATE): every edge loads its source id and
  * gathers one 8-byte value of a max_nodes vector, in the lane layout of the
  * PageRank kernel, without the row sums.  Timing it gives the speed a kernel
  * that gathers one 8-byte value per edge cannot beat on this snapshot (the
  * floor set by the L1 data path, one wavefront per distinct sector a gather
- * instruction touches).  *checksum (may be NULL) receives the sum of the
- * gathered values, to keep the work observable. */
-lg_status lg_pagerank_gather_pass(lg_snapshot* snap, double* checksum);
+ * instruction touches); time (2k passes) - (k passes) to leave out the
+ * set-up.  *checksum (may be NULL) receives the sum of the values the last
+ * pass gathered, to keep the work observable. */
+lg_status lg_pagerank_gather_pass(lg_snapshot* snap, int passes, double* checksum);
 
 /* BFS levels from `root`: u_sssp_bfs / ll_b_sssp_unweighted_bfs
  * (benchmark/benchmarks/sssp.h:219-300) over ll_bfs_template

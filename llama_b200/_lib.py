@@ -168,7 +168,7 @@ SIGNATURES = [
     ("lg_pagerank_pull", _INT, [_P, _INT, _D, _P]),
     ("lg_pagerank_push", _INT, [_P, _INT, _D, _P]),
     ("lg_pagerank_pull_noalloc", _INT, [_P, _INT, _D, _P]),
-    ("lg_pagerank_gather_pass", _INT, [_P, C.POINTER(_D)]),
+    ("lg_pagerank_gather_pass", _INT, [_P, _INT, C.POINTER(_D)]),
     ("lg_bfs", _INT, [_P, _I64, _P, C.POINTER(lg_bfs_result)]),
     ("lg_bfs_multi", _INT, [_P, _P, _INT, _P, _P]),
     ("lg_sssp_delta", _INT, [_P, _I64, C.c_uint32, _P, C.POINTER(lg_sssp_result)]),

@@ -403,9 +403,10 @@ __global__ void sum_doubles(const double* a, uint32_t n, double* out) {
 
 } // namespace lg
 
-extern "C" lg_status lg_pagerank_gather_pass(lg_snapshot* sn, double* checksum) {
+extern "C" lg_status lg_pagerank_gather_pass(lg_snapshot* sn, int passes, double* checksum) {
 	clear_error();
 	if (!sn) return set_error(LG_EINVAL, "null snapshot");
+	if (passes < 1) return set_error(LG_EINVAL, "passes must be positive");
 	FlatCsr* f = sn->flat[1];
 	if (!f) return set_error(LG_ESTATE, "flatten the in-CSR first (lg_snapshot_flatten)");
 	lg_store* s = sn->store;
@@ -421,15 +422,20 @@ extern "C" lg_status lg_pagerank_gather_pass(lg_snapshot* sn, double* checksum) 
 			nullptr);
 	s->launches++;
 	if (f->ntiles > 0) {
-		pr_gather_floor<<<flat_sweep_blocks(f->ntiles), kFlatWarps * 32, 0, st>>>(
-				f->ids.as<uint32_t>(), (uint32_t)f->E, f->ntiles, x, part);
-		sum_doubles<<<1, 1024, 0, st>>>(part, f->ntiles, part + f->ntiles);
-		s->launches += 2;
-	} else {
-		LG_CUDA(cudaMemsetAsync(part, 0, sizeof(double), st), "memset");
+		for (int p = 0; p < passes; p++)
+			pr_gather_floor<<<flat_sweep_blocks(f->ntiles), kFlatWarps * 32, 0, st>>>(
+					f->ids.as<uint32_t>(), (uint32_t)f->E, f->ntiles, x, part);
+		s->launches += passes;
 	}
 	LG_CUDA(cudaGetLastError(), "pr_gather_floor");
 	if (checksum) {
+		if (f->ntiles > 0) {
+			sum_doubles<<<1, 1024, 0, st>>>(part, f->ntiles, part + f->ntiles);
+			s->launches++;
+		} else {
+			LG_CUDA(cudaMemsetAsync(part, 0, sizeof(double), st), "memset");
+		}
+		LG_CUDA(cudaGetLastError(), "sum");
 		LG_CUDA(cudaMemcpyAsync(checksum, part + (f->ntiles > 0 ? f->ntiles : 0), sizeof(double),
 				cudaMemcpyDeviceToHost, st), "d2h");
 		LG_CUDA(cudaStreamSynchronize(st), "gather pass");

@@ -426,16 +426,16 @@ class Snapshot:
         check(fn(self._h, ptr(src), len(src), ptr(res)))
         return res
 
-    def gather_pass(self):
-        """One pass of the PageRank iteration's loads alone over the flat
-        in-CSR (``lg_pagerank_gather_pass``); returns the checksum."""
+    def gather_pass(self, passes=1):
+        """`passes` passes of the PageRank iteration's loads alone over the
+        flat in-CSR (``lg_pagerank_gather_pass``); returns the checksum."""
         c = C.c_double()
-        check(lib.lg_pagerank_gather_pass(self._h, C.byref(c)))
+        check(lib.lg_pagerank_gather_pass(self._h, int(passes), C.byref(c)))
         return c.value
 
-    def gather_pass_async(self):
+    def gather_pass_async(self, passes=1):
         """The same without reading the checksum back (for timing)."""
-        check(lib.lg_pagerank_gather_pass(self._h, None))
+        check(lib.lg_pagerank_gather_pass(self._h, int(passes), None))
 
     def autotune(self, names=None):
         """Measure the launch parameters `names` (TUNABLES keys, default all)

@@ -149,6 +149,7 @@ def test_gather_pass_checksum_and_state():
                 sn.gather_pass()
             sn.flatten(1)
             got = sn.gather_pass()
+            assert sn.gather_pass(3) == got            # every pass gathers the same
             off, nb = sn.adjacency(1)
             od = sn.out_degrees().astype(np.float64)
             want = float(np.sum((1.0 / sn.max_nodes) / od[nb]))

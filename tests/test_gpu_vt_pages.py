@@ -54,9 +54,31 @@ def paged_levels(hg):
     return descs, keep, shared
 
 
+def block_levels():
+    """Level 0 = a seeded R-MAT graph minus 30 % of the edges among vertices
+    below 2048; levels 1-3 add those back in thirds and each deletes 2 % of
+    the other level-0 edges of that block, so every level changes the vertex
+    tables of the first four pages only and the later pages stay shared."""
+    g0 = HostGraph.from_spec(workloads.rmat_single_level(scale=14, seed=3))
+    src, dst = g0.level_input(0)[:2]
+    rng = np.random.default_rng(7)
+    block = (src < 2048) & (dst < 2048)
+    held = block & (rng.random(len(src)) < 0.3)
+    part = rng.integers(1, 4, len(src))
+    gone = np.zeros(len(src), bool)
+    hg = HostGraph(g0.max_nodes)
+    hg.add_level(src[~held], dst[~held])
+    for l in (1, 2, 3):
+        cand = np.flatnonzero(block & ~held & ~gone)
+        d = rng.choice(cand, max(1, len(cand) // 50), replace=False)
+        gone[d] = True
+        add = held & (part == l)
+        hg.add_level(src[add], dst[add], src[np.sort(d)], dst[np.sort(d)])
+    return hg
+
+
 def test_page_table_ingest_equals_flat_ingest():
-    spec = workloads.rmat_multiversion(scale=14, seed=3, levels=6, level0=0.9, delete=0.003)
-    hg = HostGraph.from_spec(spec)
+    hg = block_levels()
     descs, keep, shared = paged_levels(hg)
     assert shared > 0                                   # pages really are shared
     with Store() as flat, Store() as paged:
