@@ -91,36 +91,6 @@ __device__ __forceinline__ bool bsearch_u32(const uint32_t* base, uint32_t n, ui
 	return lo < n && __ldg(base + lo) == x;
 }
 
-// Common elements of two sorted lists A (na) and B (nb) by one thread: a
-// merge when na + nb steps are fewer than na binary searches, else a binary
-// search per element of A whose lower end only moves forward (A is sorted).
-__device__ __forceinline__ uint32_t intersect_lane(const uint32_t* A, uint32_t na,
-		const uint32_t* B, uint32_t nb) {
-	uint32_t c = 0;
-	if (na + nb <= na * (32u - __clz(nb | 1u))) {
-		uint32_t i = 0, j = 0;
-		while (i < na && j < nb) {
-			const uint32_t x = __ldg(A + i), y = __ldg(B + j);
-			c += x == y;
-			i += x <= y;
-			j += y <= x;
-		}
-		return c;
-	}
-	uint32_t lo0 = 0;
-	for (uint32_t i = 0; i < na && lo0 < nb; i++) {
-		const uint32_t x = __ldg(A + i);
-		uint32_t lo = lo0, hi = nb;
-		while (lo < hi) {
-			const uint32_t mid = (lo + hi) >> 1;
-			if (__ldg(B + mid) < x) lo = mid + 1; else hi = mid;
-		}
-		c += lo < nb && __ldg(B + lo) == x;
-		lo0 = lo;
-	}
-	return c;
-}
-
 constexpr uint32_t kTcSmall = 16;   // lists this short are intersected by one lane
 
 __global__ void __launch_bounds__(kTcThreads)
@@ -142,7 +112,9 @@ tc_count(const unsigned long long* keys, const uint32_t* adj, uint64_t m, const 
 		}
 		// (sa, la) is now the shorter list
 		const bool small = la <= kTcSmall;
-		if (e < m && small) c += intersect_lane(adj + sa, la, adj + sb, lb);
+		if (e < m && small)
+			for (uint32_t j = 0; j < la; j++)
+				c += bsearch_u32(adj + sb, lb, __ldg(adj + sa + j));
 		unsigned big = __ballot_sync(0xffffffffu, e < m && !small);
 		while (big) {
 			const int src = __ffs(big) - 1;
