@@ -546,7 +546,11 @@ lg_status lg_adjoint_free(lg_adjoint* tape);
 /* Multi-source BFS and batched BC bottom-up steps: in-degree above which a
  * warp, not a thread, scans a vertex's in-edges, default 512. */
 #define LG_TUNE_MS_HEAVY        4
-#define LG_TUNE_COUNT           5
+/* PageRank's tile kernel (LG_TUNE_PR_CTAS_PER_SM = 0): 8 = the build whose
+ * registers are capped for 8 resident CTAs (64 warps) per SM; any other
+ * value = the build the compiler sizes freely (default 0). */
+#define LG_TUNE_PR_TILE_OCC     5
+#define LG_TUNE_COUNT           6
 #define LG_TUNE_MAX_DEVICES     64
 lg_status lg_tune_get(int device, int key, int64_t* value);
 lg_status lg_tune_set(int device, int key, int64_t value);

@@ -93,6 +93,9 @@ extern "C" lg_status lg_autotune(lg_snapshot* sn, unsigned keys, lg_tune_trial* 
 	if ((keys & (1u << LG_TUNE_PR_CTAS_PER_SM)) && sn->in.present)
 		probes.push_back({LG_TUNE_PR_CTAS_PER_SM, {0, 4, 5, 6},
 			[=]() { return lg_pagerank_pull(sn, 6, 0.85, dout); }});
+	if ((keys & (1u << LG_TUNE_PR_TILE_OCC)) && sn->in.present)
+		probes.push_back({LG_TUNE_PR_TILE_OCC, {0, 8},
+			[=]() { return lg_pagerank_pull(sn, 6, 0.85, dout); }});
 	if ((keys & (1u << LG_TUNE_PPR_KTILE)) && want_ppr)
 		probes.push_back({LG_TUNE_PPR_KTILE, {32, 64, 128, 256},
 			[=, &seeds]() { return lg_ppr(one, 1, seeds.data(), 256, 4, 0.85, dout); }});

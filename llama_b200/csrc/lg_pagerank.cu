@@ -81,6 +81,13 @@ pr_flat_step(FlatTiles a, PrOp op) {
 	flat_sweep_tile(a, op, rowsum);
 }
 
+// The same with registers capped for 8 resident CTAs (64 warps) per SM.
+__global__ void __launch_bounds__(kFlatWarps * 32, 8)
+pr_flat_step_occ8(FlatTiles a, PrOp op) {
+	__shared__ double rowsum[kFlatWarps][kFlatTile];
+	flat_sweep_tile(a, op, rowsum);
+}
+
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kFlatWarps * 32, kMinBlocks)
 pr_flat_loop(FlatTiles a, PrOp op) {
@@ -316,6 +323,7 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 	s->launches += 2;
 	const unsigned fix_blocks = flat_fixup_blocks(ntiles);   // a thread per tile boundary
 	const int ctas = (int)tune_value(s->device, LG_TUNE_PR_CTAS_PER_SM);
+	const bool occ8 = tune_value(s->device, LG_TUNE_PR_TILE_OCC) == 8;
 	int sms = 148;
 	if (ctas > 0) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
 	for (int it = 0; it < iterations; it++) {
@@ -323,8 +331,8 @@ extern "C" lg_status lg_pagerank_pull(lg_snapshot* sn, int iterations,
 		op.contrib_next = (it & 1) ? c0 : c1;
 		op.pr_out = (it == iterations - 1) ? pr_buf : nullptr;
 		if (ntiles > 0) {
-			launch_flat_sweep(a, op, sms, ctas, st, pr_flat_step, pr_flat_loop<4>,
-					pr_flat_loop<6>, pr_flat_loop<8>);
+			launch_flat_sweep(a, op, sms, ctas, st, occ8 ? pr_flat_step_occ8 : pr_flat_step,
+					pr_flat_loop<4>, pr_flat_loop<6>, pr_flat_loop<8>);
 			s->launches++;
 		}
 		if (ntiles > 1) {

@@ -22,6 +22,7 @@ const Limits kLimits[LG_TUNE_COUNT] = {
 	{256, 16384, 2048}, // LG_TUNE_PPR_RANGE
 	{256, 16384, 1024}, // LG_TUNE_SSSP_RANGE
 	{32, 1u << 20, 512},// LG_TUNE_MS_HEAVY
+	{0, 8, 0},          // LG_TUNE_PR_TILE_OCC (0 or 8)
 };
 
 std::mutex g_mu;

@@ -269,7 +269,8 @@ TUNABLES = {"pr_ctas_per_sm": _lib.LG_TUNE_PR_CTAS_PER_SM,
             "ppr_ktile": _lib.LG_TUNE_PPR_KTILE,
             "ppr_range": _lib.LG_TUNE_PPR_RANGE,
             "sssp_range": _lib.LG_TUNE_SSSP_RANGE,
-            "ms_heavy": _lib.LG_TUNE_MS_HEAVY}
+            "ms_heavy": _lib.LG_TUNE_MS_HEAVY,
+            "pr_tile_occ": _lib.LG_TUNE_PR_TILE_OCC}
 
 
 def tune_set(device, name, value):

@@ -36,6 +36,9 @@ def test_every_value_gives_the_same_results(store):
             tune_set(0, "pr_ctas_per_sm", c)
             assert np.array_equal(sn.pagerank_pull(7, 0.85), pr0)
         tune_reset(0)
+        tune_set(0, "pr_tile_occ", 8)
+        assert np.array_equal(sn.pagerank_pull(7, 0.85), pr0)
+        tune_reset(0)
         for kt in (32, 64, 128):
             tune_set(0, "ppr_ktile", kt)
             assert np.array_equal(ppr([sn], seeds, iterations=5), x0)
@@ -61,7 +64,8 @@ def test_autotune_keeps_the_fastest_measured_value(store):
     tune_reset(0)
     with store.snapshot() as sn:
         res = sn.autotune()
-    assert set(res) == {"pr_ctas_per_sm", "ppr_ktile", "ppr_range", "sssp_range", "ms_heavy"}
+    assert set(res) == {"pr_ctas_per_sm", "ppr_ktile", "ppr_range", "sssp_range", "ms_heavy",
+                        "pr_tile_occ"}
     for name, r in res.items():
         assert r["chosen"] in r["ms"]
         assert all(ms > 0 for ms in r["ms"].values())
