@@ -68,15 +68,11 @@ struct AffOp {
 		for (int i = 0; i < kFlatPerLane; i++)
 			v[i] = id[i] != kNoId ? __dmul_rn(wv[i], __ldg(x + id[i])) : 0.0;
 	}
-	struct Row { uint32_t v; };
-	__device__ __forceinline__ Row load_row(uint32_t k) const { return Row{__ldg(nz_rows + k)}; }
-	__device__ __forceinline__ double finish_row(const Row& r, double s) const {
-		const double yv = __dadd_rn(__ldg(base + r.v), __dmul_rn(d, s));
-		y[r.v] = yv;
-		return fabs(yv - __ldg(x + r.v));
-	}
 	__device__ __forceinline__ double finish(uint32_t k, double s) const {
-		return finish_row(load_row(k), s);
+		const uint32_t v = __ldg(nz_rows + k);
+		const double yv = __dadd_rn(__ldg(base + v), __dmul_rn(d, s));
+		y[v] = yv;
+		return fabs(yv - __ldg(x + v));
 	}
 	__device__ __forceinline__ void residual(double r) const { atomicAdd(resid, r); }
 };

@@ -19,8 +19,6 @@
 //                                            (id = kNoId past the end)
 //   double finish(k, s) const                row k (index into nz_rows) has
 //                                            sum s; returns its residual term
-//   Row    load_row(k) const                 what finish needs of row k,
-//   double finish_row(row, s) const          loaded early, and finish with it
 //   void   residual(r) const                 one warp's residual total
 //   static constexpr bool kResidual          finish() returns something
 #ifndef LG_FLAT_SWEEP_CUH_
@@ -88,10 +86,6 @@ __device__ __forceinline__ double flat_sweep_one(const FlatTiles& a, const Op& o
 		for (int i = 0; i < kFlatPerLane; i++)
 			id[i] = eb + i < a.E ? __ldcs(a.ids + eb + i) : kNoId;
 	}
-	// the first 32 rows' metadata is loaded now, while the gathers are in
-	// flight, instead of after the sums
-	const uint32_t seg0 = __ldg(a.tile_seg + t);
-	const typename Op::Row pre = op.load_row(min(seg0 + lane, a.R > 0 ? a.R - 1 : 0u));
 	double x[kFlatPerLane];
 	op.values(eb, id, x);
 
@@ -149,9 +143,9 @@ __device__ __forceinline__ double flat_sweep_one(const FlatTiles& a, const Op& o
 	}
 	__syncwarp();
 	const uint32_t done = (H > 0 && !closes) ? H - 1 : H;
+	const uint32_t seg0 = __ldg(a.tile_seg + t);
 	double res = 0.0;
-	if (lane < done) res += op.finish_row(pre, rs[lane]);
-	for (uint32_t r = lane + 32u; r < done; r += 32u) res += op.finish(seg0 + r, rs[r]);
+	for (uint32_t r = lane; r < done; r += 32u) res += op.finish(seg0 + r, rs[r]);
 	return res;
 }
 

@@ -64,18 +64,13 @@ struct PrOp {
 		for (int i = 0; i < kFlatPerLane; i++)
 			x[i] = id[i] != kNoId ? __ldg(contrib + id[i]) : 0.0;
 	}
-	struct Row { uint32_t v, dg; };
-	__device__ __forceinline__ Row load_row(uint32_t k) const {
-		return Row{__ldg(nz_rows + k), __ldg(nz_outdeg + k)};
-	}
-	__device__ __forceinline__ double finish_row(const Row& r, double s) const {
-		const double pr = __dadd_rn(base, __dmul_rn(d, s));
-		contrib_next[r.v] = r.dg ? pr / (double)r.dg : 0.0;
-		if (pr_out) pr_out[r.v] = pr;
-		return 0.0;
-	}
 	__device__ __forceinline__ double finish(uint32_t k, double s) const {
-		return finish_row(load_row(k), s);
+		const uint32_t v = __ldg(nz_rows + k);
+		const double pr = __dadd_rn(base, __dmul_rn(d, s));
+		const uint32_t dg = __ldg(nz_outdeg + k);
+		contrib_next[v] = dg ? pr / (double)dg : 0.0;
+		if (pr_out) pr_out[v] = pr;
+		return 0.0;
 	}
 	__device__ __forceinline__ void residual(double) const {}
 };
