@@ -373,7 +373,8 @@ def run_lg(args):
     tuning = None
     if not args.no_autotune:
         t0 = time.time()
-        tuning = sn.autotune(["pr_ctas_per_sm", "pr_tile_occ", "ms_heavy", "sssp_range"])
+        tuning = sn.autotune(["pr_ctas_per_sm", "pr_tile_occ", "ms_heavy", "sssp_split",
+                              "sssp_range"])
         tuning["seconds"] = time.time() - t0
 
     pr_dev = torch.empty(V, dtype=torch.float64, device=f"cuda:{local}")

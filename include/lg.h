@@ -550,7 +550,14 @@ lg_status lg_adjoint_free(lg_adjoint* tape);
  * registers are capped for 8 resident CTAs (64 warps) per SM; any other
  * value = the build the compiler sizes freely (default 0). */
 #define LG_TUNE_PR_TILE_OCC     5
-#define LG_TUNE_COUNT           6
+/* Delta-stepping SSSP: 1 = the rounds of a bucket relax only the light edges
+ * (weight < delta) of the near queue and the vertices settled in the bucket
+ * relax their heavy edges once when it drains, over a copy of the snapshot's
+ * out-CSR split per row (built on the first call for a delta, 8 bytes per
+ * live edge, kept with the snapshot); 0 = every round relaxes every edge of
+ * the near queue.  Default 1. */
+#define LG_TUNE_SSSP_SPLIT      6
+#define LG_TUNE_COUNT           7
 #define LG_TUNE_MAX_DEVICES     64
 lg_status lg_tune_get(int device, int key, int64_t* value);
 lg_status lg_tune_set(int device, int key, int64_t value);

@@ -107,6 +107,11 @@ extern "C" lg_status lg_autotune(lg_snapshot* sn, unsigned keys, lg_tune_trial* 
 			[=, &roots]() {
 				return lg_sssp_delta(sn, roots[0], 32, (uint32_t*)iout, nullptr);
 			}});
+	if ((keys & (1u << LG_TUNE_SSSP_SPLIT)) && weighted)
+		probes.push_back({LG_TUNE_SSSP_SPLIT, {0, 1},
+			[=, &roots]() {
+				return lg_sssp_delta(sn, roots[0], 32, (uint32_t*)iout, nullptr);
+			}});
 	if ((keys & (1u << LG_TUNE_MS_HEAVY)) && sn->in.present)
 		probes.push_back({LG_TUNE_MS_HEAVY, {128, 256, 512, 1024, 4096},
 			[=, &roots]() {

@@ -246,9 +246,15 @@ struct lg_store {
 struct lg_adjoint_maps;
 void lg_free_adjoint_maps(lg_adjoint_maps* m);
 
+// The snapshot's out-edges split by weight for delta-stepping (lg_sssp.cu);
+// built on first use for a delta, freed with the snapshot.
+struct lg_sssp_split;
+void lg_free_sssp_split(lg_sssp_split* p);
+
 struct lg_snapshot {
 	lg_store* store = nullptr;
 	lg_adjoint_maps* adj_maps = nullptr;
+	lg_sssp_split* sssp_split = nullptr;
 	lg::FlatCsr* flat[2] = {nullptr, nullptr};   // lg_snapshot_flatten, per direction
 	int level = 0;
 	int min_level = 0;          // oldest level the snapshot sees

@@ -19,6 +19,9 @@
 #include "lg_flat.cuh"
 #include "lg_tune.h"
 
+#include <cstring>
+#include <new>
+
 namespace lg {
 
 constexpr uint32_t kInf = LG_UNREACHED;
@@ -142,6 +145,73 @@ sssp_split_far(const uint32_t* far, unsigned long long n,
 	if ((threadIdx.x & 31) == 0 && m != ~0ull) atomicMin(ctr + 2, m);
 }
 
+// ---------------------------------------------------------------------------
+// Light / heavy split.  Edges lighter than delta can improve a vertex inside
+// the current bucket, heavier ones only in later buckets, so the rounds of a
+// bucket relax only the light edges of the near queue, and each vertex
+// settled in the bucket relaxes its heavy edges once when the bucket drains
+// (Meyer & Sanders' light/heavy phases).  The flat out-CSR is partitioned per
+// row, light edges first (stable), and two one-fragment-per-vertex views
+// point at the light and the heavy part of every row.
+// ---------------------------------------------------------------------------
+
+// Row v of the flat out-CSR (off, ids, w) rewritten light-first into
+// (ids2, w2); lc[v] = its light edges.  A warp per row: a counting pass,
+// then a writing pass, 32 edges at a time with ballots (stable).
+__global__ void sssp_partition(const uint32_t* off, const uint32_t* ids, const uint32_t* w,
+		uint64_t V, uint32_t delta, uint32_t* ids2, uint32_t* w2, uint2* lfr, uint2* hfr) {
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+	for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < V; v += nwarps) {
+		const uint32_t b = __ldg(off + v), e = __ldg(off + v + 1);
+		uint32_t nl = 0;
+		for (uint32_t k = b + lane; k < e + ((32u - (e - b) % 32u) % 32u); k += 32) {
+			const bool light = k < e && __ldg(w + k) < delta;
+			nl += __popc(__ballot_sync(0xffffffffu, light));
+		}
+		uint32_t pl = b, ph = b + nl;
+		const uint32_t below = (1u << lane) - 1u;
+		for (uint32_t k = b + lane; k < e + ((32u - (e - b) % 32u) % 32u); k += 32) {
+			const bool in = k < e;
+			const uint32_t wk = in ? __ldg(w + k) : 0u;
+			const uint32_t ik = in ? __ldg(ids + k) : 0u;
+			const bool light = in && wk < delta;
+			const unsigned lm = __ballot_sync(0xffffffffu, light);
+			const unsigned hm = __ballot_sync(0xffffffffu, in && !light);
+			if (light) { const uint32_t d = pl + __popc(lm & below); ids2[d] = ik; w2[d] = wk; }
+			else if (in) { const uint32_t d = ph + __popc(hm & below); ids2[d] = ik; w2[d] = wk; }
+			pl += __popc(lm);
+			ph += __popc(hm);
+		}
+		if (lane == 0) {
+			lfr[v] = make_uint2(b, nl << kLevelBits);
+			hfr[v] = make_uint2(b + nl, (e - b - nl) << kLevelBits);
+		}
+	}
+}
+
+__global__ void sssp_iota(uint32_t* a, uint64_t n) {
+	const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+	if (i < n) a[i] = (uint32_t)i;
+}
+
+// The vertices of the near queue join the bucket's settled list once each
+// (stamp = bucket number); ctr[3] counts the list.
+__global__ void sssp_collect(const uint32_t* q, uint32_t n, uint32_t* bstamp, uint32_t bucket,
+		uint32_t* blist, unsigned long long* ctr) {
+	__shared__ uint32_t sbuf[kSsspThreads / 32][kPushBuf];
+	const uint32_t wid = threadIdx.x >> 5;
+	uint32_t nn = 0;
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	const uint64_t end = ((uint64_t)n + 31) & ~31ull;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+		const uint32_t v = i < n ? q[i] : 0u;
+		const bool take = i < n && atomicExch(bstamp + v, bucket) != bucket;
+		wq_add(take, v, sbuf[wid], nn, blist, ctr + 3);
+	}
+	wq_flush(sbuf[wid], nn, blist, ctr + 3);
+}
+
 __global__ void sssp_reach(const uint32_t* dist, const uint32_t* outdeg, uint64_t V,
 		unsigned long long* ctr) {
 	unsigned long long c = 0, e = 0, mx = 0;
@@ -166,6 +236,84 @@ __global__ void sssp_reach(const uint32_t* dist, const uint32_t* outdeg, uint64_
 
 using namespace lg;
 
+struct lg_sssp_split {
+	uint32_t delta = 0;
+	DevBuf ids, w;          // E: the flat out-CSR, each row light edges first
+	DevBuf lfr, hfr;        // V: one fragment per row, light part / heavy part
+	DevBuf fidx;            // V + 1: fragment index of every row (the identity)
+	DevBuf zeros;           // deletion bitset of the view (none deleted)
+	DevBuf lt_light, lt_heavy;   // device LevelTabs of the two views
+	SnapCsr view(bool heavy, const uint32_t* deg, uint64_t V) const {
+		SnapCsr c;
+		c.frag_off = fidx.as<uint32_t>();
+		c.frags = (heavy ? hfr : lfr).as<uint2>();
+		c.lt = (heavy ? lt_heavy : lt_light).as<LevelTab>();
+		c.deg = deg;
+		c.V = V;
+		return c;
+	}
+};
+
+void lg_free_sssp_split(lg_sssp_split* p) { delete p; }
+
+namespace {
+
+// The snapshot's out-CSR flattened (the snapshot's own flat CSR when it has
+// one with weights, else one built here and dropped after) and split for
+// `delta`; kept on the snapshot for the next call with the same delta.
+lg_status ensure_split(lg_snapshot* sn, uint32_t delta) {
+	if (sn->sssp_split && sn->sssp_split->delta == delta) return LG_OK;
+	lg_store* s = sn->store;
+	cudaStream_t st = s->stream;
+	const uint64_t V = sn->V;
+	lg_sssp_split* p = sn->sssp_split;
+	if (!p) {
+		p = new (std::nothrow) lg_sssp_split();
+		if (!p) return set_error(LG_ENOMEM, "host allocation");
+		sn->sssp_split = p;
+	}
+	p->delta = 0;
+	FlatCsr own;
+	const FlatCsr* f = sn->flat[0];
+	if (!f || !f->weighted) {
+		LG_TRY(build_flat(sn, 0, own, false));
+		if (!own.weighted) return set_error(LG_ESTATE, "the out-CSR carries no edge weights");
+		f = &own;
+	}
+	const uint64_t E = f->E;
+	LG_TRY(p->ids.reserve(std::max<uint64_t>(E, 1) * 4));
+	LG_TRY(p->w.reserve(std::max<uint64_t>(E, 1) * 4));
+	LG_TRY(p->lfr.reserve(std::max<uint64_t>(V, 1) * sizeof(uint2)));
+	LG_TRY(p->hfr.reserve(std::max<uint64_t>(V, 1) * sizeof(uint2)));
+	LG_TRY(p->fidx.reserve((V + 1) * 4));
+	const uint64_t words = E / 32 + 2;
+	LG_TRY(p->zeros.reserve(words * 4));
+	LG_TRY(p->lt_light.reserve(sizeof(LevelTab)));
+	LG_TRY(p->lt_heavy.reserve(sizeof(LevelTab)));
+	LG_CUDA(cudaMemsetAsync(p->zeros.p, 0, words * 4, st), "memset");
+	int sms = 148;
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+	sssp_partition<<<(unsigned)sms * 16u, 256, 0, st>>>(f->off.as<uint32_t>(),
+			f->ids.as<uint32_t>(), f->w.as<uint32_t>(), V, delta, p->ids.as<uint32_t>(),
+			p->w.as<uint32_t>(), p->lfr.as<uint2>(), p->hfr.as<uint2>());
+	sssp_iota<<<grid_for(V + 1, 256), 256, 0, st>>>(p->fidx.as<uint32_t>(), V + 1);
+	LG_CUDA(cudaGetLastError(), "sssp_partition");
+	s->launches += 2;
+	LevelTab lt;
+	memset(&lt, 0, sizeof(lt));
+	lt.ids[0] = p->ids.as<uint32_t>();
+	lt.w[0] = p->w.as<uint32_t>();
+	lt.del[0] = p->zeros.as<uint32_t>();
+	LG_CUDA(cudaMemcpyAsync(p->lt_light.p, &lt, sizeof(lt), cudaMemcpyHostToDevice, st), "h2d");
+	LG_CUDA(cudaMemcpyAsync(p->lt_heavy.p, &lt, sizeof(lt), cudaMemcpyHostToDevice, st), "h2d");
+	LG_CUDA(cudaStreamSynchronize(st), "sssp split");    // `own` and `lt` go out of scope
+	s->h2d_bytes += 2 * sizeof(lt);
+	p->delta = delta;
+	return LG_OK;
+}
+
+} // namespace
+
 extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta,
 		uint32_t* dist, lg_sssp_result* result) {
 	clear_error();
@@ -186,7 +334,7 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 	LG_TRY(sc[2].reserve(V * 4));          // far pile
 	LG_TRY(sc[3].reserve(V * 4));          // far pile being compacted
 	LG_TRY(sc[5].reserve(2 * V * 4));      // near and far stamps
-	LG_TRY(sc[6].reserve(8 * sizeof(unsigned long long)));
+	LG_TRY(sc[6].reserve(8 * sizeof(unsigned long long)));     // counters (4 used)
 	LG_TRY(sc[7].reserve((2 * V + 1) * 4));   // queue slot counts and their prefix
 	uint32_t* qcnt = sc[7].as<uint32_t>();
 	uint32_t* qpos = qcnt + V;
@@ -206,17 +354,58 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 	unsigned long long* ctr = sc[6].as<unsigned long long>();
 	// the one-fragment view of a flattened out-CSR when there is one
 	const FlatCsr* fo = sn->flat[0];
-	const SnapCsr out = (fo && fo->has_view && fo->weighted)
+	SnapCsr out = (fo && fo->has_view && fo->weighted)
 			? fo->view(sn->out.deg.as<uint32_t>()) : sn->view(0);
+	// light / heavy split (LG_TUNE_SSSP_SPLIT): rounds walk the light view,
+	// the bucket's settled list walks the heavy view once
+	const bool split = tune_value(s->device, LG_TUNE_SSSP_SPLIT) != 0;
+	SnapCsr heavy = out;
+	uint32_t* blist = nullptr;
+	uint32_t* bstamp = nullptr;
+	if (split) {
+		LG_TRY(ensure_split(sn, delta));
+		out = sn->sssp_split->view(false, sn->out.deg.as<uint32_t>(), V);
+		heavy = sn->sssp_split->view(true, sn->out.deg.as<uint32_t>(), V);
+		LG_TRY(sc[9].reserve(V * 4));
+		LG_TRY(sc[10].reserve(V * 4));
+		blist = sc[9].as<uint32_t>();
+		bstamp = sc[10].as<uint32_t>();
+		LG_CUDA(cudaMemsetAsync(bstamp, 0xff, V * 4, st), "memset");
+	}
 
 	sssp_init<<<grid_for(V, 256), 256, 0, st>>>(d, stamp, fstamp, V, (uint32_t)root, q);
 	LG_CUDA(cudaGetLastError(), "sssp_init");
 	s->launches++;
-	uint64_t qlen = 1, flen = 0, relaxations = 0;
-	uint32_t hi = delta, round = 0, epoch = 0;
+	uint64_t qlen = 1, flen = 0, blen = 0, relaxations = 0;
+	uint32_t hi = delta, round = 0, epoch = 0, bid = 0;
 	int buckets = 1;
-	unsigned long long h[3];
-	while (qlen > 0 || flen > 0) {
+	unsigned long long h[4];
+	LG_CUDA(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned long long), st), "memset");
+	while (qlen > 0 || flen > 0 || blen > 0) {
+		if (qlen == 0 && blen > 0) {
+			// the bucket has drained: its settled vertices relax their
+			// heavy edges once (every such relaxation lands at >= hi, in
+			// the far pile)
+			round++;
+			unsigned long long init[4] = {0, flen, 0, 0};
+			LG_CUDA(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st), "h2d");
+			s->h2d_bytes += sizeof(init);
+			list_slots<<<grid_for(blen, 256), 256, 0, st>>>(heavy, blist, (uint32_t)blen, qcnt);
+			LG_TRY(exclusive_scan_u32(qcnt, qpos, blen, sc[8], st, nullptr));
+			sssp_relax<<<relax_blocks, kSsspThreads, 0, st>>>(heavy, blist, qpos, (uint32_t)blen,
+					d, stamp, fstamp, round, epoch, hi, qn, far, ctr, range);
+			LG_CUDA(cudaGetLastError(), "sssp_relax heavy");
+			s->launches += 5;
+			LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+			LG_CUDA(cudaStreamSynchronize(st), "sssp heavy");
+			s->d2h_bytes += sizeof(h);
+			if (h[0] != 0 || h[1] > V) return set_error(LG_ECUDA, "sssp heavy phase out of bounds");
+			flen = h[1];
+			relaxations += h[2];
+			blen = 0;
+			bid++;
+			continue;
+		}
 		if (qlen == 0) {
 			// near queue drained: split the far pile at the next bound; if
 			// nothing falls below it, jump to the bucket of the smallest
@@ -226,7 +415,7 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 			for (int attempt = 0; attempt < 2; attempt++) {
 				round++;
 				epoch++;
-				unsigned long long init[3] = {0, 0, ~0ull};
+				unsigned long long init[4] = {0, 0, ~0ull, 0};
 				LG_CUDA(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st), "h2d");
 				s->h2d_bytes += sizeof(init);
 				const unsigned split_blocks = (unsigned)std::min<uint64_t>(
@@ -235,7 +424,8 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 						fstamp, round, epoch, lo, hi, q, far2, ctr);
 				LG_CUDA(cudaGetLastError(), "sssp_split_far");
 				s->launches++;
-				LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+				LG_CUDA(cudaMemcpyAsync(h, ctr, 3 * sizeof(unsigned long long),
+						cudaMemcpyDeviceToHost, st), "d2h");
 				LG_CUDA(cudaStreamSynchronize(st), "sssp split");
 				s->d2h_bytes += sizeof(h);
 				if (h[0] > V || h[1] > V) return set_error(LG_ECUDA, "sssp queue overflow");
@@ -251,9 +441,14 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 			continue;
 		}
 		round++;
-		unsigned long long init[3] = {0, flen, 0};
+		unsigned long long init[4] = {0, flen, 0, blen};
 		LG_CUDA(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st), "h2d");
 		s->h2d_bytes += sizeof(init);
+		if (split) {
+			sssp_collect<<<(unsigned)std::min<uint64_t>(grid_for(qlen, kSsspThreads), relax_blocks),
+					kSsspThreads, 0, st>>>(q, (uint32_t)qlen, bstamp, bid, blist, ctr);
+			s->launches++;
+		}
 		list_slots<<<grid_for(qlen, 256), 256, 0, st>>>(out, q, (uint32_t)qlen, qcnt);
 		LG_TRY(exclusive_scan_u32(qcnt, qpos, qlen, sc[8], st, nullptr));
 		sssp_relax<<<relax_blocks, kSsspThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, d,
@@ -267,6 +462,8 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 		qlen = h[0];
 		flen = h[1];
 		relaxations += h[2];
+		if (split) blen = h[3];
+		if (blen > V) return set_error(LG_ECUDA, "sssp settled list overflow");
 		std::swap(q, qn);
 	}
 	LG_CUDA(cudaMemsetAsync(ctr, 0, 3 * sizeof(unsigned long long), st), "memset");

@@ -986,6 +986,7 @@ lg_status lg_snapshot_close(lg_snapshot* sn) {
 	cudaStreamSynchronize(sn->store->stream);
 	sn->store->open_snapshots--;
 	if (sn->adj_maps) lg_free_adjoint_maps(sn->adj_maps);
+	if (sn->sssp_split) lg_free_sssp_split(sn->sssp_split);
 	for (int d = 0; d < 2; d++) lg_flat_release(sn->store, sn->flat[d]);
 	// keep this snapshot's device buffers for the next open
 	lg_store* s = sn->store;

@@ -270,7 +270,8 @@ TUNABLES = {"pr_ctas_per_sm": _lib.LG_TUNE_PR_CTAS_PER_SM,
             "ppr_range": _lib.LG_TUNE_PPR_RANGE,
             "sssp_range": _lib.LG_TUNE_SSSP_RANGE,
             "ms_heavy": _lib.LG_TUNE_MS_HEAVY,
-            "pr_tile_occ": _lib.LG_TUNE_PR_TILE_OCC}
+            "pr_tile_occ": _lib.LG_TUNE_PR_TILE_OCC,
+            "sssp_split": _lib.LG_TUNE_SSSP_SPLIT}
 
 
 def tune_set(device, name, value):

@@ -58,6 +58,14 @@ def test_every_value_gives_the_same_results(store):
             tune_set(0, "sssp_range", r)
             assert np.array_equal(sn.sssp(int(roots[0]), 32)[0], d0)
         tune_reset(0)
+        tune_set(0, "sssp_split", 0)
+        for r in roots[:4]:
+            a = sn.sssp(int(r), 32)[0]
+            tune_set(0, "sssp_split", 1)
+            assert np.array_equal(sn.sssp(int(r), 32)[0], a)
+            assert np.array_equal(sn.sssp(int(r), 7)[0], a)        # another delta
+            tune_set(0, "sssp_split", 0)
+        tune_reset(0)
 
 
 def test_autotune_keeps_the_fastest_measured_value(store):
@@ -65,7 +73,7 @@ def test_autotune_keeps_the_fastest_measured_value(store):
     with store.snapshot() as sn:
         res = sn.autotune()
     assert set(res) == {"pr_ctas_per_sm", "ppr_ktile", "ppr_range", "sssp_range", "ms_heavy",
-                        "pr_tile_occ"}
+                        "pr_tile_occ", "sssp_split"}
     for name, r in res.items():
         assert r["chosen"] in r["ms"]
         assert all(ms > 0 for ms in r["ms"].values())
