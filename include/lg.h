@@ -555,7 +555,7 @@ lg_status lg_adjoint_free(lg_adjoint* tape);
  * relax their heavy edges once when it drains, over a copy of the snapshot's
  * out-CSR split per row (built on the first call for a delta, 8 bytes per
  * live edge, kept with the snapshot); 0 = every round relaxes every edge of
- * the near queue.  Default 1. */
+ * the near queue.  Default 0 (measured faster on the R-MAT workloads). */
 #define LG_TUNE_SSSP_SPLIT      6
 #define LG_TUNE_COUNT           7
 #define LG_TUNE_MAX_DEVICES     64
