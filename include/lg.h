@@ -296,8 +296,9 @@ lg_status lg_snapshot_adjacency(lg_snapshot* snap, int dir, uint64_t* offsets,
  * (ll_t_flatten, benchmark/tools/flatten.h).  Later traversals of that
  * direction on this snapshot (lg_pagerank_pull; lg_bfs top-down for dir 0,
  * bottom-up for dir 1) read the flat CSR instead of walking fragments and
- * deletion bits; results are unchanged.  Holds about 4 B per live edge plus
- * 20 B per vertex of device memory until lg_snapshot_unflatten or
+ * deletion bits; results are unchanged.  Holds about 4 B per live edge (8 B
+ * for the out direction of a weighted store, which keeps the weights for
+ * SSSP) plus 20 B per vertex of device memory until lg_snapshot_unflatten or
  * lg_snapshot_close, which hand it back to the store: the store keeps up to
  * two released flat CSRs for later flattens (freed by lg_store_destroy).
  * A no-op if the direction is already flat.  LG_ESTATE if dir is 1 and the

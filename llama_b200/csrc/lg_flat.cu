@@ -195,8 +195,10 @@ lg_status build_flat(lg_snapshot* sn, int dir, FlatCsr& f, bool view) {
 	const uint64_t V = sn->V;
 	const unsigned B = 256;
 	const DevCsr& csr = dir == 0 ? s->out : s->in;
-	bool weighted = true;
-	for (int l = sn->min_level; l <= sn->level; l++)
+	// edge weights are read only along out-edges (SSSP), so only the out
+	// direction carries them into the flat CSR
+	bool weighted = dir == 0;
+	for (int l = sn->min_level; l <= sn->level && weighted; l++)
 		if (csr.levels[l]->n_fragment_slots > 0 && !csr.levels[l]->w.p) weighted = false;
 
 	f.V = V;
