@@ -8,6 +8,7 @@
 // probes write into device buffers of their own, so the snapshot and the
 // caller's data are untouched; every value computes the same results.
 #include "lg_device.cuh"
+#include "lg_flat.cuh"
 #include "lg_tune.h"
 
 #include <algorithm>
@@ -89,6 +90,27 @@ extern "C" lg_status lg_autotune(lg_snapshot* sn, unsigned keys, lg_tune_trial* 
 	double* dout = out.as<double>();
 	int32_t* iout = out.as<int32_t>();
 	lg_snapshot* one[1] = {sn};
+	// PageRank's sweeps and the multi-source bottom-up steps that read
+	// LG_TUNE_MS_HEAVY run over the flat in-CSR: a snapshot without one gets
+	// one for the probes (so a PageRank probe times the sweeps, not a flatten
+	// per call) and gives it back when they end.  Without the memory for it
+	// the PageRank probes build their own per call and the MS_HEAVY probe,
+	// whose threshold only the flat kernels read, is skipped.
+	const unsigned in_keys = (1u << LG_TUNE_PR_CTAS_PER_SM) | (1u << LG_TUNE_PR_TILE_OCC) |
+			(1u << LG_TUNE_MS_HEAVY);
+	struct FlatGuard {
+		lg_snapshot* sn = nullptr;
+		~FlatGuard() {
+			if (!sn) return;
+			cudaStreamSynchronize(sn->store->stream);
+			lg_flat_release(sn->store, sn->flat[1]);
+			sn->flat[1] = nullptr;
+		}
+	} made_in;
+	if ((keys & in_keys) && sn->in.present && !sn->flat[1]) {
+		if (lg_snapshot_flatten(sn, 1) == LG_OK) made_in.sn = sn;
+		else clear_error();
+	}
 	std::vector<Probe> probes;
 	if ((keys & (1u << LG_TUNE_PR_CTAS_PER_SM)) && sn->in.present)
 		probes.push_back({LG_TUNE_PR_CTAS_PER_SM, {0, 4, 5, 6},
@@ -112,7 +134,7 @@ extern "C" lg_status lg_autotune(lg_snapshot* sn, unsigned keys, lg_tune_trial* 
 			[=, &roots]() {
 				return lg_sssp_delta(sn, roots[0], 32, (uint32_t*)iout, nullptr);
 			}});
-	if ((keys & (1u << LG_TUNE_MS_HEAVY)) && sn->in.present)
+	if ((keys & (1u << LG_TUNE_MS_HEAVY)) && sn->flat[1])
 		probes.push_back({LG_TUNE_MS_HEAVY, {128, 256, 512, 1024, 4096},
 			[=, &roots]() {
 				return lg_bfs_multi(sn, roots.data(), (int)roots.size(), iout, nullptr);

@@ -50,9 +50,11 @@ def test_every_value_gives_the_same_results(store):
             assert np.array_equal(x == 0, ~nz)
             assert np.max(np.abs(x[nz] - x0[nz]) / x0[nz]) <= 1e-12
         tune_reset(0)
+        sn.flatten(1)                     # the threshold is read by the flat bottom-up kernels
         for h in (32, 128, 4096):
             tune_set(0, "ms_heavy", h)
             assert np.array_equal(sn.bfs_multi(roots)[0], lv0)
+        sn.unflatten()
         tune_reset(0)
         for r in (256, 512, 4096):
             tune_set(0, "sssp_range", r)
@@ -72,6 +74,8 @@ def test_autotune_keeps_the_fastest_measured_value(store):
     tune_reset(0)
     with store.snapshot() as sn:
         res = sn.autotune()
+        # the flat in-CSR made for the probes is released again
+        assert not sn.is_flat(1)
     assert set(res) == {"pr_ctas_per_sm", "ppr_ktile", "ppr_range", "sssp_range", "ms_heavy",
                         "pr_tile_occ", "sssp_split"}
     for name, r in res.items():
@@ -79,4 +83,16 @@ def test_autotune_keeps_the_fastest_measured_value(store):
         assert all(ms > 0 for ms in r["ms"].values())
         assert r["ms"][r["chosen"]] == min(r["ms"].values())
         assert tune_get(0, name) == r["chosen"]
+    tune_reset(0)
+
+
+def test_autotune_leaves_a_flat_snapshot_flat(store):
+    """A snapshot that was flat before the probes stays flat after them."""
+    tune_reset(0)
+    with store.snapshot() as sn:
+        sn.flatten(1)
+        res = sn.autotune(["ms_heavy"])
+        assert sn.is_flat(1)
+    assert set(res) == {"ms_heavy"}
+    assert res["ms_heavy"]["ms"][res["ms_heavy"]["chosen"]] == min(res["ms_heavy"]["ms"].values())
     tune_reset(0)
