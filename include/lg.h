@@ -533,9 +533,9 @@ lg_status lg_adjoint_free(lg_adjoint* tape);
  * rejected with LG_EINVAL; every value gives the same results, only the
  * speed changes.
  * ------------------------------------------------------------------------- */
-/* Flat-CSR sweeps (PageRank pull, the adjoint's solves): resident CTAs per
- * SM of a persistent sweep, each warp looping over 256-edge tiles; 0 = one
- * CTA per 8 tiles, each warp one tile. */
+/* Flat-CSR sweeps (PageRank pull, the adjoint's solves): resident CTAs (of
+ * 8 warps) per SM of a persistent sweep, each warp looping over 256-edge
+ * tiles; 0 = one CTA per 4 tiles, each warp one tile. */
 #define LG_TUNE_PR_CTAS_PER_SM  0
 /* Personalized PageRank: columns per pass (a multiple of 32; the K columns
  * run in passes of this many, each pass all iterations), default 256. */
@@ -548,7 +548,7 @@ lg_status lg_adjoint_free(lg_adjoint* tape);
  * warp, not a thread, scans a vertex's in-edges, default 512. */
 #define LG_TUNE_MS_HEAVY        4
 /* PageRank's tile kernel (LG_TUNE_PR_CTAS_PER_SM = 0): 8 = the build whose
- * registers are capped for 8 resident CTAs (64 warps) per SM; any other
+ * registers are capped for 64 resident warps per SM; any other
  * value = the build the compiler sizes freely (default 0). */
 #define LG_TUNE_PR_TILE_OCC     5
 /* Delta-stepping SSSP: 1 = the rounds of a bucket relax only the light edges
@@ -573,7 +573,12 @@ lg_status lg_tune_reset(int device);
  * others without an in-CSR) are skipped, and so are the PPR ones when three
  * max_nodes x 256 FP64 blocks do not fit in half of the free device memory.  trials (may be NULL)
  * receives one entry per candidate measured, up to max_trials; n_trials the
- * count.  Allocates its own probe buffers; the snapshot is not changed. */
+ * count.  Allocates its own probe buffers; the snapshot is not changed.  The
+ * PageRank and multi-source BFS probes run over the flat in-CSR: when the
+ * snapshot has none, one is made for them (lg_snapshot_flatten's memory)
+ * and released when the probes end; where it does not fit, the PageRank
+ * probes flatten per call and LG_TUNE_MS_HEAVY, read only by the flat
+ * bottom-up kernels, is skipped. */
 typedef struct lg_tune_trial {
 	int32_t key;
 	int32_t chosen;    /* 1 for the value kept */

@@ -84,9 +84,9 @@ aff_flat_step(FlatTiles a, AffOp op) {
 }
 
 template <int kMinBlocks>
-__global__ void __launch_bounds__(kFlatWarps * 32, kMinBlocks)
+__global__ void __launch_bounds__(kFlatLoopWarps * 32, kMinBlocks)
 aff_flat_loop(FlatTiles a, AffOp op) {
-	__shared__ double rowsum[kFlatWarps][kFlatTile];
+	__shared__ double rowsum[kFlatLoopWarps][kFlatTile];
 	flat_sweep_loop(a, op, rowsum);
 }
 

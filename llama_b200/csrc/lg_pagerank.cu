@@ -81,17 +81,17 @@ pr_flat_step(FlatTiles a, PrOp op) {
 	flat_sweep_tile(a, op, rowsum);
 }
 
-// The same with registers capped for 8 resident CTAs (64 warps) per SM.
-__global__ void __launch_bounds__(kFlatWarps * 32, 8)
+// The same with registers capped for 64 resident warps per SM.
+__global__ void __launch_bounds__(kFlatWarps * 32, 64 / kFlatWarps)
 pr_flat_step_occ8(FlatTiles a, PrOp op) {
 	__shared__ double rowsum[kFlatWarps][kFlatTile];
 	flat_sweep_tile(a, op, rowsum);
 }
 
 template <int kMinBlocks>
-__global__ void __launch_bounds__(kFlatWarps * 32, kMinBlocks)
+__global__ void __launch_bounds__(kFlatLoopWarps * 32, kMinBlocks)
 pr_flat_loop(FlatTiles a, PrOp op) {
-	__shared__ double rowsum[kFlatWarps][kFlatTile];
+	__shared__ double rowsum[kFlatLoopWarps][kFlatTile];
 	flat_sweep_loop(a, op, rowsum);
 }
 
