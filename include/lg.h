@@ -380,7 +380,13 @@ lg_status lg_pagerank_gather_pass(lg_snapshot* snap, int passes, double* checksu
  * result (may be NULL): reached = number of reached vertices, the "bfs_count"
  * result (benchmark/benchmarks/bfs.h:117-127); reach_edges = sum of the
  * out-degrees of the reached vertices (the Graph500 edge count used for
- * GTEPS); max_level; and how many steps ran top-down and bottom-up. */
+ * GTEPS); max_level; and how many steps ran top-down and bottom-up.
+ * With the snapshot's in-CSR flat (lg_snapshot_flatten(snap, 1)), or a store
+ * without one, the whole traversal is one cooperative launch whose CTAs
+ * choose each level's direction on the device and meet at bounded grid
+ * barriers (LG_TUNE_BFS_LEVELS; LG_ETIMEOUT if a barrier wait runs out);
+ * otherwise a launch sequence per level with the direction chosen on the
+ * host.  Both make the same choices and give the same result. */
 typedef struct lg_bfs_result {
 	uint64_t reached;
 	uint64_t reach_edges;
@@ -558,7 +564,12 @@ lg_status lg_adjoint_free(lg_adjoint* tape);
  * live edge, kept with the snapshot); 0 = every round relaxes every edge of
  * the near queue.  Default 0 (measured faster on the R-MAT workloads). */
 #define LG_TUNE_SSSP_SPLIT      6
-#define LG_TUNE_COUNT           7
+/* One-root BFS (lg_bfs) with the snapshot's in-CSR flat (or no in-CSR):
+ * 1 = every level in one cooperative launch whose CTAs choose the direction
+ * on the device and meet at grid barriers; 0 = a launch sequence per level
+ * with the direction chosen on the host.  Default 1. */
+#define LG_TUNE_BFS_LEVELS      7
+#define LG_TUNE_COUNT           8
 #define LG_TUNE_MAX_DEVICES     64
 lg_status lg_tune_get(int device, int key, int64_t* value);
 lg_status lg_tune_set(int device, int key, int64_t value);
@@ -567,18 +578,19 @@ lg_status lg_tune_reset(int device);
 /* The autotuner: for every tunable whose bit (1u << key) is set in `keys`,
  * sets each candidate value on the snapshot's GPU in turn, times the call
  * that reads it on this snapshot (a warm-up call, then the median of three
- * timed with CUDA events; PageRank pull, PPR with 256 seeds, SSSP and
- * multi-source BFS from vertices of the snapshot), and keeps the fastest.
+ * timed with CUDA events; PageRank pull, PPR with 256 seeds, SSSP,
+ * multi-source BFS and four one-root BFS from vertices of the snapshot), and
+ * keeps the fastest.
  * Tunables that the snapshot cannot exercise (SSSP without weights, the
  * others without an in-CSR) are skipped, and so are the PPR ones when three
  * max_nodes x 256 FP64 blocks do not fit in half of the free device memory.  trials (may be NULL)
  * receives one entry per candidate measured, up to max_trials; n_trials the
  * count.  Allocates its own probe buffers; the snapshot is not changed.  The
- * PageRank and multi-source BFS probes run over the flat in-CSR: when the
- * snapshot has none, one is made for them (lg_snapshot_flatten's memory)
- * and released when the probes end; where it does not fit, the PageRank
- * probes flatten per call and LG_TUNE_MS_HEAVY, read only by the flat
- * bottom-up kernels, is skipped. */
+ * PageRank and BFS probes run over the flat in-CSR: when the snapshot has
+ * none, one is made for them (lg_snapshot_flatten's memory) and released
+ * when the probes end; where it does not fit, the PageRank probes flatten
+ * per call and LG_TUNE_MS_HEAVY and LG_TUNE_BFS_LEVELS, read only with a
+ * flat in-CSR, are skipped. */
 typedef struct lg_tune_trial {
 	int32_t key;
 	int32_t chosen;    /* 1 for the value kept */

@@ -39,7 +39,8 @@ LG_TUNE_SSSP_RANGE = 3
 LG_TUNE_MS_HEAVY = 4
 LG_TUNE_PR_TILE_OCC = 5
 LG_TUNE_SSSP_SPLIT = 6
-LG_TUNE_COUNT = 7
+LG_TUNE_BFS_LEVELS = 7
+LG_TUNE_COUNT = 8
 LG_TUNE_MAX_DEVICES = 64
 
 

@@ -90,14 +90,15 @@ extern "C" lg_status lg_autotune(lg_snapshot* sn, unsigned keys, lg_tune_trial* 
 	double* dout = out.as<double>();
 	int32_t* iout = out.as<int32_t>();
 	lg_snapshot* one[1] = {sn};
-	// PageRank's sweeps and the multi-source bottom-up steps that read
-	// LG_TUNE_MS_HEAVY run over the flat in-CSR: a snapshot without one gets
+	// PageRank's sweeps, the multi-source bottom-up steps that read
+	// LG_TUNE_MS_HEAVY and the one-launch BFS run over the flat in-CSR: a
+	// snapshot without one gets
 	// one for the probes (so a PageRank probe times the sweeps, not a flatten
 	// per call) and gives it back when they end.  Without the memory for it
-	// the PageRank probes build their own per call and the MS_HEAVY probe,
-	// whose threshold only the flat kernels read, is skipped.
+	// the PageRank probes build their own per call and the MS_HEAVY and
+	// BFS_LEVELS probes, whose values only the flat kernels read, are skipped.
 	const unsigned in_keys = (1u << LG_TUNE_PR_CTAS_PER_SM) | (1u << LG_TUNE_PR_TILE_OCC) |
-			(1u << LG_TUNE_MS_HEAVY);
+			(1u << LG_TUNE_MS_HEAVY) | (1u << LG_TUNE_BFS_LEVELS);
 	struct FlatGuard {
 		lg_snapshot* sn = nullptr;
 		~FlatGuard() {
@@ -138,6 +139,13 @@ extern "C" lg_status lg_autotune(lg_snapshot* sn, unsigned keys, lg_tune_trial* 
 		probes.push_back({LG_TUNE_MS_HEAVY, {128, 256, 512, 1024, 4096},
 			[=, &roots]() {
 				return lg_bfs_multi(sn, roots.data(), (int)roots.size(), iout, nullptr);
+			}});
+	if ((keys & (1u << LG_TUNE_BFS_LEVELS)) && (sn->flat[1] || !sn->in.present))
+		probes.push_back({LG_TUNE_BFS_LEVELS, {0, 1},
+			[=, &roots]() {
+				lg_status r = LG_OK;
+				for (int i = 0; i < 4 && !r; i++) r = lg_bfs(sn, roots[i * 16], iout, nullptr);
+				return r;
 			}});
 	int nt = 0;
 	for (const Probe& p : probes) {

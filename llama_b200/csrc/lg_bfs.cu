@@ -14,6 +14,11 @@
 
 namespace lg {
 
+// lg_bfs_levels.cu: the whole BFS in one cooperative launch; *ran = false
+// when it does not apply to the snapshot (nothing launched).
+lg_status bfs_levels_run(lg_snapshot* sn, uint32_t root, int32_t* lvl, lg_bfs_result* result,
+		bool* ran);
+
 constexpr int32_t kUnreached = LG_UNREACHED;
 constexpr int kBfsThreads = 256;
 constexpr uint32_t kBfsRange = 1024;
@@ -287,6 +292,16 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 	if (!dev_out) {
 		LG_TRY(sc[4].reserve(V * 4));
 		lvl = sc[4].as<int32_t>();
+	}
+	// the whole traversal in one cooperative launch where it applies
+	bool ran = false;
+	LG_TRY(bfs_levels_run(sn, (uint32_t)root, lvl, result, &ran));
+	if (ran) {
+		if (!dev_out) {
+			LG_TRY(copy_out(s, levels, lvl, V * 4));
+			LG_CUDA(cudaStreamSynchronize(st), "bfs");
+		}
+		return LG_OK;
 	}
 	uint32_t* q = sc[0].as<uint32_t>();
 	uint32_t* nq = sc[1].as<uint32_t>();

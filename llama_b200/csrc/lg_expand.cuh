@@ -24,8 +24,20 @@ namespace lg {
 
 constexpr int kUnroll = 4;
 
+// Loads of the list and its offsets (kLd): 0 = through the read-only path
+// (the default); 1 = through L2, for a kernel that rewrites them between its
+// own phases (the read-only path may hold lines from before the rewrite);
+// 2 = plain generic loads, for offsets kept in shared memory.
+template <int kLd>
+__device__ __forceinline__ uint32_t ld_list(const uint32_t* p) {
+	if (kLd == 0) return __ldg(p);
+	if (kLd == 1) return __ldcg(p);
+	return *p;
+}
+
 // First index e in [0, m] with arr[e] >= x (arr sorted, arr[m] the total),
 // computed by the whole warp with 32-way probing.
+template <int kLd = 0>
 __device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t* arr, uint32_t m,
 		uint32_t x) {
 	const uint32_t lane = threadIdx.x & 31u;
@@ -33,7 +45,7 @@ __device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t* arr, uint32
 	while (hi - lo > 32) {
 		const uint32_t step = (hi - lo + 31) / 32;
 		uint32_t p = lo + lane * step;
-		bool below = p < hi && __ldg(arr + p) < x;
+		bool below = p < hi && ld_list<kLd>(arr + p) < x;
 		unsigned b = __ballot_sync(0xffffffffu, below);
 		uint32_t c = __popc(b);              // probes below x: lanes 0..c-1
 		uint32_t nlo = c ? lo + (c - 1) * step + 1 : lo;
@@ -43,7 +55,7 @@ __device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t* arr, uint32
 		hi = nhi;
 	}
 	uint32_t p = lo + lane;
-	bool below = p < hi && __ldg(arr + p) < x;
+	bool below = p < hi && ld_list<kLd>(arr + p) < x;
 	return lo + __popc(__ballot_sync(0xffffffffu, below));
 }
 
@@ -58,6 +70,7 @@ struct Window {
 	uint32_t lo, hi;   // slots covered by the whole window
 };
 
+template <int kLd = 0>
 __device__ __forceinline__ Window load_window(const SnapCsr& g, const uint32_t* list,
 		const uint32_t* pos, uint32_t ew, uint32_t e_end, uint32_t a, uint32_t b) {
 	const uint32_t lane = threadIdx.x & 31u;
@@ -66,10 +79,10 @@ __device__ __forceinline__ Window load_window(const SnapCsr& g, const uint32_t* 
 	w.valid = w.e < e_end;
 	w.v = 0; w.f0 = 0; w.start = 0; w.s0 = 0; w.s1 = 0;
 	if (w.valid) {
-		w.v = list ? __ldg(list + w.e) : w.e;
+		w.v = list ? ld_list<kLd>(list + w.e) : w.e;
 		w.f0 = __ldg(g.frag_off + w.v);
-		w.start = __ldg(pos + w.e);
-		const uint32_t end = __ldg(pos + w.e + 1);
+		w.start = ld_list<kLd>(pos + w.e);
+		const uint32_t end = ld_list<kLd>(pos + w.e + 1);
 		w.s0 = max(w.start, a);
 		w.s1 = min(end, b);
 		if (w.s1 < w.s0) w.s1 = w.s0;
@@ -115,15 +128,16 @@ __device__ __forceinline__ void locate_slot(const SnapCsr& g, const Window& w,
 // Entries of range [a, b): e_begin includes an entry that started before a
 // and reaches into the range; e_end stops before entries starting at or
 // after b (for the last range, b covers the whole list).
+template <int kLd = 0>
 __device__ __forceinline__ void range_entries(const uint32_t* pos, uint32_t n,
 		uint32_t a, uint32_t b, bool last_range, uint32_t* e_begin, uint32_t* e_end) {
-	uint32_t eb = warp_lower_bound(pos, n, a);
-	if (eb > 0 && (eb == n || __ldg(pos + eb) > a)) {
+	uint32_t eb = warp_lower_bound<kLd>(pos, n, a);
+	if (eb > 0 && (eb == n || ld_list<kLd>(pos + eb) > a)) {
 		// the entry before eb may straddle a
-		if (__ldg(pos + eb) > a || eb == n) eb--;
+		if (ld_list<kLd>(pos + eb) > a || eb == n) eb--;
 	}
 	*e_begin = eb;
-	*e_end = last_range ? n : warp_lower_bound(pos, n, b);
+	*e_end = last_range ? n : warp_lower_bound<kLd>(pos, n, b);
 }
 
 // Process range `r` of a list's slot space (ranges of `range` slots, nranges
@@ -133,7 +147,7 @@ __device__ __forceinline__ void range_entries(const uint32_t* pos, uint32_t n,
 // lanes are non-decreasing across a chunk and lanes past the window's last
 // slot get owner lane 31, so owner_lane is a safe key for segmented
 // reductions (owner_vertex of such lanes is a placeholder).
-template <class Body>
+template <int kLd = 0, class Body>
 __device__ __forceinline__ void range_for_each(const SnapCsr& g, const uint32_t* list,
 		const uint32_t* pos, uint32_t n, uint32_t total, uint32_t nranges,
 		uint32_t range, uint32_t r, Body&& body) {
@@ -142,10 +156,10 @@ __device__ __forceinline__ void range_for_each(const SnapCsr& g, const uint32_t*
 	const uint32_t ra = r * range;
 	const uint32_t rb = last_range ? total : min(total, ra + range);
 	uint32_t e_begin, e_end;
-	range_entries(pos, n, ra, rb, last_range, &e_begin, &e_end);
+	range_entries<kLd>(pos, n, ra, rb, last_range, &e_begin, &e_end);
 	const LevelTab* lt = g.lt;
 	for (uint32_t ew = e_begin; ew < e_end; ew += 32) {
-		const Window w = load_window(g, list, pos, ew, e_end, ra, rb);
+		const Window w = load_window<kLd>(g, list, pos, ew, e_end, ra, rb);
 		for (uint32_t base = w.lo; base < w.hi; base += 32 * kUnroll) {
 			uint32_t nb[kUnroll], own[kUnroll], lvs[kUnroll], ids[kUnroll];
 			bool act[kUnroll];

@@ -271,7 +271,8 @@ TUNABLES = {"pr_ctas_per_sm": _lib.LG_TUNE_PR_CTAS_PER_SM,
             "sssp_range": _lib.LG_TUNE_SSSP_RANGE,
             "ms_heavy": _lib.LG_TUNE_MS_HEAVY,
             "pr_tile_occ": _lib.LG_TUNE_PR_TILE_OCC,
-            "sssp_split": _lib.LG_TUNE_SSSP_SPLIT}
+            "sssp_split": _lib.LG_TUNE_SSSP_SPLIT,
+            "bfs_levels": _lib.LG_TUNE_BFS_LEVELS}
 
 
 def tune_set(device, name, value):
