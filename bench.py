@@ -752,17 +752,28 @@ def extras(args, st, stream, device, parity):
         try:
             V, E = sn.max_nodes, sn.num_edges
             res = {}
-            # one-root direction-optimising BFS, the 16 bench roots one call each
+            # one-root direction-optimising BFS, the 16 bench roots one call each,
+            # over the flat in-CSR (made once, timed apart): every level of a
+            # root in one cooperative launch
             broots = workloads.pick_roots(sn.out_degrees(), args.roots, seed=3)
+            _, flat_ms = _timed(stream, lambda: sn.flatten(1))
             lv1 = torch.empty(V, dtype=torch.int32, device=dev)
             sn.bfs(int(broots[0]), out=lv1)
-            ms, reach = 0.0, 0
-            for r in broots:
+            multi = torch.empty((len(broots), V), dtype=torch.int32, device=dev)
+            sn.bfs_multi(broots, out=multi)
+            ms, reach, same = 0.0, 0, True
+            for i, r in enumerate(broots):
                 (_, rr), t = _timed(stream, lambda: sn.bfs(int(r), out=lv1))
                 ms += t
                 reach += rr.reach_edges
+                same = same and bool(torch.equal(lv1, multi[i]))
+            del multi
+            parity["bfs_single_root_ok"] = same   # equals the step's multi-source rows
             res["bfs_single_root"] = {
                 "roots": len(broots), "ms": ms, "gteps": reach / (ms / 1e3) / 1e9,
+                "flatten_in_csr_ms": flat_ms,
+                "mode": "lg_bfs over the flat in-CSR: all levels of a root in one cooperative "
+                        "launch (LG_TUNE_BFS_LEVELS = 1)",
                 "roofline": roof(8 * reach + 4 * V * len(broots), ms,
                                  "sum over roots of 4 B id + 4 B neighbour level per reached "
                                  "out-edge + 4 B level per vertex",

@@ -192,15 +192,10 @@ __device__ __forceinline__ uint32_t lv_range(uint32_t total, uint32_t nwarps) {
 	return min(max(r, 32u), kLvMaxRange);
 }
 
-__global__ void bfs_levels_init(int32_t* level, uint64_t V, uint32_t root, uint32_t* q0,
-		uint32_t* bits0, uint32_t* bits1, const uint32_t* outdeg, LvCtl* c) {
-	const uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-	if (v < V) level[v] = v == root ? 0 : kLvUnreached;
-	if (v < (V + 31) / 32) {
-		bits0[v] = v == (root >> 5) ? 1u << (root & 31u) : 0u;
-		bits1[v] = 0u;
-	}
-	if (v == 0) {
+// Resets the control block and queues the root; bfs_levels fills the level
+// array and the first two bitmaps itself.
+__global__ void bfs_levels_init(uint32_t root, uint32_t* q0, const uint32_t* outdeg, LvCtl* c) {
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
 		q0[0] = root;
 		for (int i = 0; i < 3; i++)
 			for (int j = 0; j < 4; j++) c->ctr[i][j] = 0;
@@ -234,6 +229,17 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 	long long list_len = -1;          // unfound rows of the last bottom-up level, -1: none
 	bool list_in_fcnt = false;        // that list is in fcnt (else in fpos)
 	int32_t td = 0, bu = 0, cur = 0;
+	{
+		// levels: 0 at the root, unreached elsewhere; bitmap 0 = {root},
+		// bitmap 1 clear (level 0's next frontier)
+		const uint32_t root = __ldcg(q0);
+		for (uint32_t v = gtid; v < V; v += nthreads) level[v] = v == root ? 0 : kLvUnreached;
+		for (uint32_t w = gtid; w < W; w += nthreads) {
+			bits0[w] = w == (root >> 5) ? 1u << (root & 31u) : 0u;
+			bits1[w] = 0u;
+		}
+		if (!grid_barrier(c)) return;
+	}
 	for (;; cur++) {
 		unsigned long long* now = c->ctr[cur % 3];
 		unsigned long long* nxt = c->ctr[(cur + 1) % 3];
@@ -563,8 +569,7 @@ lg_status bfs_levels_run(lg_snapshot* sn, uint32_t root, int32_t* lvl, lg_bfs_re
 	LvCtl* ctl = sc[9].as<LvCtl>();
 	unsigned long long* bsum = reinterpret_cast<unsigned long long*>(
 			sc[9].as<unsigned char>() + sizeof(LvCtl));
-	bfs_levels_init<<<grid_for(V, 256), 256, 0, st>>>(lvl, V, root, q0, bits0, bits1, outdeg,
-			ctl);
+	bfs_levels_init<<<1, 32, 0, st>>>(root, q0, outdeg, ctl);
 	LG_CUDA(cudaGetLastError(), "bfs_levels_init");
 	void* args[] = {&out, &nz_rows, &nz_off, &R, &E, &in_ids, &outdeg, &V32, &out_edges,
 			&has_in, &lvl, &q0, &q1, &bits0, &bits1, &bits2, &fcnt, &fpos, &bsum, &ctl};
