@@ -265,11 +265,9 @@ extern "C" lg_status lg_bc(lg_snapshot* sn, const int64_t* sources, int n_source
 				hlist, hcount);
 		s->launches++;
 	}
-	// one pinned word pair for the per-level counters
+	// the store's pinned words for the per-level counters
 	unsigned long long* hc = nullptr;
-	LG_CUDA(cudaHostAlloc((void**)&hc, 2 * sizeof(unsigned long long), cudaHostAllocDefault),
-			"cudaHostAlloc");
-	struct PinnedFree { unsigned long long* p; ~PinnedFree() { cudaFreeHost(p); } } pf{hc};
+	LG_TRY(host_words(s, &hc));
 	int sms = 148;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
 	const unsigned grid = (unsigned)sms * 8u;

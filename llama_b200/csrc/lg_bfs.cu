@@ -318,8 +318,7 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 	LG_CUDA(cudaGetLastError(), "bfs_init");
 	s->launches++;
 	unsigned long long h[2];
-	LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
-	LG_CUDA(cudaStreamSynchronize(st), "bfs");
+	LG_TRY(read_words(s, ctr, 2, h));
 	uint64_t qlen = 1, mf = h[1];
 	uint64_t mu = sn->out.n_edges - mf;   // edges out of unvisited vertices
 	uint64_t reached = 1, reach_edges = mf;
@@ -365,9 +364,7 @@ extern "C" lg_status lg_bfs(lg_snapshot* sn, int64_t root, int32_t* levels,
 			s->launches += 2;
 		}
 		LG_CUDA(cudaGetLastError(), "bfs step");
-		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
-		s->d2h_bytes += sizeof(h);
-		LG_CUDA(cudaStreamSynchronize(st), "bfs step");
+		LG_TRY(read_words(s, ctr, 2, h));
 		qlen = h[0];
 		mf = h[1];
 		mu -= std::min(mu, (uint64_t)mf);

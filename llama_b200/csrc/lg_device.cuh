@@ -215,6 +215,8 @@ struct lg_store {
 	// pinned staging for host -> device copies (two halves, double-buffered)
 	void* pinned = nullptr;
 	size_t pinned_bytes = 0;
+	// a few pinned words for per-step counters read back by the host loops
+	unsigned long long* host_words = nullptr;
 	cudaEvent_t staged[2] = {nullptr, nullptr};
 	// scratch shared by the analytics calls of this store
 	lg::DevBuf scratch[12];
@@ -286,6 +288,14 @@ lg_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n,
 // Copy `bytes` of device data to a caller buffer (host or device) on the
 // store's stream, counting host-bound bytes.
 lg_status copy_out(lg_store* s, void* dst, const void* src, size_t bytes);
+
+// The store's kHostWords pinned words (allocated on first use), for
+// counters a host loop reads back every step.
+constexpr int kHostWords = 16;
+lg_status host_words(lg_store* s, unsigned long long** words);
+// Waits for the store's stream and reads n <= 8 device words into out through
+// pinned words 8..15 (words 0..7 stay with the caller).
+lg_status read_words(lg_store* s, const unsigned long long* dev, int n, unsigned long long* out);
 
 // A DevLevel for direction dir (0 out, 1 in) of a new level: the store's
 // spare (buffers of the last dropped level) or a new one.  Null if the host

@@ -729,9 +729,7 @@ extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int 
 		LG_CUDA(cudaGetLastError(), "bcm_roots");
 		s->launches++;
 		unsigned long long h[3];
-		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
-		LG_CUDA(cudaStreamSynchronize(st), "bc batched");
-		s->d2h_bytes += sizeof(h);
+		LG_TRY(read_words(s, ctr, 3, h));
 		std::vector<uint64_t> qoff = {0, h[0]};   // level k's queue: [qoff[k], qoff[k+1])
 		uint64_t mf = h[1];
 		uint64_t mu = sn->out.n_edges > mf ? sn->out.n_edges - mf : 0;
@@ -758,8 +756,7 @@ extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int 
 				ms_top_down<<<grid, kMsThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, lk, seen,
 						nxt, cand, ctr + 3);
 				unsigned long long nc = 0;
-				LG_CUDA(cudaMemcpyAsync(&nc, ctr + 3, sizeof(nc), cudaMemcpyDeviceToHost, st), "d2h");
-				LG_CUDA(cudaStreamSynchronize(st), "bc batched");
+				LG_TRY(read_words(s, ctr + 3, 1, &nc));
 				if (nc > 0)
 					ms_commit<<<grid_for(nc, kMsThreads * kCommitPer), kMsThreads, 0, st>>>(cand,
 							(uint32_t)nc, k + 1, V, n, nxt,
@@ -788,9 +785,7 @@ extern "C" lg_status lg_bc_batched(lg_snapshot* sn, const int64_t* sources, int 
 				s->launches++;
 			}
 			LG_CUDA(cudaGetLastError(), "bc batched forward");
-			LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
-			LG_CUDA(cudaStreamSynchronize(st), "bc batched");
-			s->d2h_bytes += sizeof(h) + sizeof(unsigned long long);
+			LG_TRY(read_words(s, ctr, 3, h));
 			if (has_in && h[0] > 0) {
 				// pull into the new level over its in-edges
 				list_slots<<<grid_for(h[0], B), B, 0, st>>>(in, q2, (uint32_t)h[0], qcnt);
@@ -912,9 +907,7 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 		LG_CUDA(cudaGetLastError(), "ms_roots");
 		s->launches++;
 		unsigned long long h[3];
-		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
-		LG_CUDA(cudaStreamSynchronize(st), "msbfs");
-		s->d2h_bytes += sizeof(h);
+		LG_TRY(read_words(s, ctr, 3, h));
 		uint64_t qlen = h[0];
 		uint64_t mf = h[1];        // out-degree sum of the frontier, for the direction choice
 		uint64_t mu = sn->out.n_edges > mf ? sn->out.n_edges - mf : 0;
@@ -932,8 +925,7 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 				ms_top_down<<<td_blocks, kMsThreads, 0, st>>>(out, q, qpos, (uint32_t)qlen, cur,
 						seen, nxt, cand, ctr + 3);
 				unsigned long long nc = 0;
-				LG_CUDA(cudaMemcpyAsync(&nc, ctr + 3, sizeof(nc), cudaMemcpyDeviceToHost, st), "d2h");
-				LG_CUDA(cudaStreamSynchronize(st), "msbfs step");
+				LG_TRY(read_words(s, ctr + 3, 1, &nc));
 				if (nc > 0)
 					ms_commit<<<grid_for(nc, kMsThreads * kCommitPer), kMsThreads, 0, st>>>(cand,
 							(uint32_t)nc, depth + 1, V, n, nxt,
@@ -960,9 +952,7 @@ extern "C" lg_status lg_bfs_multi(lg_snapshot* sn, const int64_t* roots, int n_r
 			ms_clear<<<grid_for(qlen, B), B, 0, st>>>(q, (uint32_t)qlen, cur);
 			LG_CUDA(cudaGetLastError(), "msbfs step");
 			s->launches++;
-			LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
-			s->d2h_bytes += sizeof(h) + sizeof(unsigned long long);
-			LG_CUDA(cudaStreamSynchronize(st), "msbfs step");
+			LG_TRY(read_words(s, ctr, 3, h));
 			qlen = h[0];
 			mf = h[1];
 			mu -= std::min(mu, (uint64_t)mf);

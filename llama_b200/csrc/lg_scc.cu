@@ -160,18 +160,14 @@ lg_status run_list_step(lg_store* s, const SnapCsr& g, const uint32_t* list, uin
 	LG_CUDA(cudaGetLastError(), "scc step");
 	s->launches += 4 + (nranges ? 1 : 0);
 	unsigned long long h = 0;
-	LG_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
-	LG_CUDA(cudaStreamSynchronize(st), "scc step");
-	s->d2h_bytes += 16;
+	LG_TRY(read_words(s, ctr, 1, &h));
 	*produced = h;
 	return LG_OK;
 }
 
 lg_status read_ctr(lg_store* s, unsigned long long* ctr, uint64_t* v) {
 	unsigned long long h = 0;
-	LG_CUDA(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, s->stream), "d2h");
-	LG_CUDA(cudaStreamSynchronize(s->stream), "scc");
-	s->d2h_bytes += 8;
+	LG_TRY(read_words(s, ctr, 1, &h));
 	*v = h;
 	return LG_OK;
 }

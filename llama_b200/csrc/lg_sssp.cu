@@ -379,7 +379,12 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 	uint64_t qlen = 1, flen = 0, blen = 0, relaxations = 0;
 	uint32_t hi = delta, round = 0, epoch = 0, bid = 0;
 	int buckets = 1;
-	unsigned long long h[4];
+	// counters read back and round set-ups written through the store's
+	// pinned words (no pageable staging on every round)
+	unsigned long long* hw = nullptr;
+	LG_TRY(host_words(s, &hw));
+	unsigned long long* h = hw;              // 4 words read back
+	unsigned long long* init = hw + 4;       // 4 words written
 	LG_CUDA(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned long long), st), "memset");
 	while (qlen > 0 || flen > 0 || blen > 0) {
 		if (qlen == 0 && blen > 0) {
@@ -387,18 +392,19 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 			// heavy edges once (every such relaxation lands at >= hi, in
 			// the far pile)
 			round++;
-			unsigned long long init[4] = {0, flen, 0, 0};
-			LG_CUDA(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st), "h2d");
-			s->h2d_bytes += sizeof(init);
+			init[0] = 0; init[1] = flen; init[2] = 0; init[3] = 0;
+			LG_CUDA(cudaMemcpyAsync(ctr, init, 4 * sizeof(unsigned long long),
+					cudaMemcpyHostToDevice, st), "h2d");
+			s->h2d_bytes += 4 * sizeof(unsigned long long);
 			list_slots<<<grid_for(blen, 256), 256, 0, st>>>(heavy, blist, (uint32_t)blen, qcnt);
 			LG_TRY(exclusive_scan_u32(qcnt, qpos, blen, sc[8], st, nullptr));
 			sssp_relax<<<relax_blocks, kSsspThreads, 0, st>>>(heavy, blist, qpos, (uint32_t)blen,
 					d, stamp, fstamp, round, epoch, hi, qn, far, ctr, range);
 			LG_CUDA(cudaGetLastError(), "sssp_relax heavy");
 			s->launches += 5;
-			LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+			LG_CUDA(cudaMemcpyAsync(h, ctr, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st), "d2h");
 			LG_CUDA(cudaStreamSynchronize(st), "sssp heavy");
-			s->d2h_bytes += sizeof(h);
+			s->d2h_bytes += 4 * sizeof(unsigned long long);
 			if (h[0] != 0 || h[1] > V) return set_error(LG_ECUDA, "sssp heavy phase out of bounds");
 			flen = h[1];
 			relaxations += h[2];
@@ -415,9 +421,10 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 			for (int attempt = 0; attempt < 2; attempt++) {
 				round++;
 				epoch++;
-				unsigned long long init[4] = {0, 0, ~0ull, 0};
-				LG_CUDA(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st), "h2d");
-				s->h2d_bytes += sizeof(init);
+				init[0] = 0; init[1] = 0; init[2] = ~0ull; init[3] = 0;
+				LG_CUDA(cudaMemcpyAsync(ctr, init, 4 * sizeof(unsigned long long),
+						cudaMemcpyHostToDevice, st), "h2d");
+				s->h2d_bytes += 4 * sizeof(unsigned long long);
 				const unsigned split_blocks = (unsigned)std::min<uint64_t>(
 						std::max<uint64_t>(grid_for(flen, kSsspThreads), 1), relax_blocks);
 				sssp_split_far<<<split_blocks, kSsspThreads, 0, st>>>(far, flen, d, stamp,
@@ -427,7 +434,7 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 				LG_CUDA(cudaMemcpyAsync(h, ctr, 3 * sizeof(unsigned long long),
 						cudaMemcpyDeviceToHost, st), "d2h");
 				LG_CUDA(cudaStreamSynchronize(st), "sssp split");
-				s->d2h_bytes += sizeof(h);
+				s->d2h_bytes += 4 * sizeof(unsigned long long);
 				if (h[0] > V || h[1] > V) return set_error(LG_ECUDA, "sssp queue overflow");
 				qlen = h[0];
 				flen = h[1];
@@ -441,9 +448,10 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 			continue;
 		}
 		round++;
-		unsigned long long init[4] = {0, flen, 0, blen};
-		LG_CUDA(cudaMemcpyAsync(ctr, init, sizeof(init), cudaMemcpyHostToDevice, st), "h2d");
-		s->h2d_bytes += sizeof(init);
+		init[0] = 0; init[1] = flen; init[2] = 0; init[3] = blen;
+		LG_CUDA(cudaMemcpyAsync(ctr, init, 4 * sizeof(unsigned long long),
+				cudaMemcpyHostToDevice, st), "h2d");
+		s->h2d_bytes += 4 * sizeof(unsigned long long);
 		if (split) {
 			sssp_collect<<<(unsigned)std::min<uint64_t>(grid_for(qlen, kSsspThreads), relax_blocks),
 					kSsspThreads, 0, st>>>(q, (uint32_t)qlen, bstamp, bid, blist, ctr);
@@ -455,9 +463,9 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 				stamp, fstamp, round, epoch, hi, qn, far, ctr, range);
 		LG_CUDA(cudaGetLastError(), "sssp_relax");
 		s->launches += 5;
-		LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
+		LG_CUDA(cudaMemcpyAsync(h, ctr, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st), "d2h");
 		LG_CUDA(cudaStreamSynchronize(st), "sssp relax");
-		s->d2h_bytes += sizeof(h);
+		s->d2h_bytes += 4 * sizeof(unsigned long long);
 		if (h[0] > V || h[1] > V) return set_error(LG_ECUDA, "sssp queue overflow");
 		qlen = h[0];
 		flen = h[1];
@@ -470,8 +478,8 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 	sssp_reach<<<592, 256, 0, st>>>(d, sn->out.deg.as<uint32_t>(), V, ctr);
 	LG_CUDA(cudaGetLastError(), "sssp_reach");
 	s->launches++;
-	LG_CUDA(cudaMemcpyAsync(h, ctr, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
-	s->d2h_bytes += sizeof(h);
+	LG_CUDA(cudaMemcpyAsync(h, ctr, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st), "d2h");
+	s->d2h_bytes += 4 * sizeof(unsigned long long);
 	if (!dev_out) LG_TRY(copy_out(s, dist, d, V * 4));
 	LG_CUDA(cudaStreamSynchronize(st), "sssp");
 	if (result) {

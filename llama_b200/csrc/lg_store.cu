@@ -95,6 +95,26 @@ static lg_status copy_out_async(lg_store* s, void* dst, const void* src, size_t 
 	return LG_OK;
 }
 
+lg_status host_words(lg_store* s, unsigned long long** words) {
+	if (!s->host_words)
+		LG_CUDA(cudaHostAlloc((void**)&s->host_words, kHostWords * sizeof(unsigned long long),
+				cudaHostAllocDefault), "cudaHostAlloc");
+	*words = s->host_words;
+	return LG_OK;
+}
+
+lg_status read_words(lg_store* s, const unsigned long long* dev, int n, unsigned long long* out) {
+	unsigned long long* hw = nullptr;
+	LG_TRY(host_words(s, &hw));
+	hw += 8;
+	LG_CUDA(cudaMemcpyAsync(hw, dev, (size_t)n * sizeof(unsigned long long),
+			cudaMemcpyDeviceToHost, s->stream), "d2h");
+	LG_CUDA(cudaStreamSynchronize(s->stream), "d2h");
+	for (int i = 0; i < n; i++) out[i] = hw[i];
+	s->d2h_bytes += (uint64_t)n * sizeof(unsigned long long);
+	return LG_OK;
+}
+
 lg_status copy_out(lg_store* s, void* dst, const void* src, size_t bytes) {
 	if (bytes == 0) return LG_OK;
 	if (s->output_mode == LG_OUTPUT_ASYNC && bytes >= LG_ASYNC_MIN_BYTES && is_pinned_host(dst))
@@ -256,10 +276,16 @@ lg_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, uint64_t n,
 			sums + tiles);
 	LG_CUDA(cudaGetLastError(), "scan launch");
 	if (total) {
-		uint64_t t = 0;
-		LG_CUDA(cudaMemcpyAsync(&t, sums + tiles, sizeof(t),
+		// read through one pinned word per host thread (kept for the
+		// thread's life): per-level loops read a total every step
+		static thread_local uint64_t* pinned_total = nullptr;
+		if (!pinned_total)
+			LG_CUDA(cudaHostAlloc((void**)&pinned_total, sizeof(uint64_t),
+					cudaHostAllocPortable), "cudaHostAlloc");
+		LG_CUDA(cudaMemcpyAsync(pinned_total, sums + tiles, sizeof(uint64_t),
 				cudaMemcpyDeviceToHost, stream), "scan total");
 		LG_CUDA(cudaStreamSynchronize(stream), "scan total");
+		const uint64_t t = *pinned_total;
 		*total = t;
 		if (t > 0xffffffffull)
 			return set_error(LG_ENOTSUP, "more than 2^32-1 fragments in a snapshot");
@@ -767,6 +793,7 @@ lg_status lg_store_destroy(lg_store* s) {
 		if (s->stage_done[i]) cudaEventDestroy(s->stage_done[i]);
 	}
 	if (s->pinned) cudaFreeHost(s->pinned);
+	if (s->host_words) cudaFreeHost(s->host_words);
 	delete s->flat_scratch;
 	for (int d = 0; d < 2; d++) {
 		delete s->flat_spare[d];
