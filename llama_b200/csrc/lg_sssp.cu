@@ -78,13 +78,19 @@ __global__ void __launch_bounds__(kSsspThreads)
 sssp_relax(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
 		uint32_t* dist, uint32_t* stamp, uint32_t* fstamp, uint32_t round, uint32_t epoch,
 		uint32_t hi, uint32_t* near_next, uint32_t* far, unsigned long long* ctr,
-		uint32_t range) {
+		uint32_t range_max) {
 	__shared__ uint32_t sbuf[kSsspThreads / 32][2][kPushBuf];
 	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
 	const uint32_t total = __ldg(pos + qlen);
-	const uint32_t nranges = (total + range - 1) / range;
 	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	// ranges of at most `range_max` slots, fewer when the queue's slots would
+	// not give every warp one: late rounds queue 10^5 - 10^6 vertices with
+	// a slot or less each, and fixed-size ranges left most warps idle while a
+	// few walked thousands of entries
+	uint32_t range = (uint32_t)(((uint64_t)total + nwarps - 1) / nwarps);
+	range = min(max((range + 31u) & ~31u, 32u), range_max);
+	const uint32_t nranges = (total + range - 1) / range;
 	unsigned long long relax = 0;
 	uint32_t nn = 0, nf = 0;       // staged near / far appends of this warp
 	for (uint32_t r = warp; r < nranges; r += nwarps) {
