@@ -26,6 +26,7 @@ namespace lg {
 
 constexpr uint32_t kInf = LG_UNREACHED;
 constexpr int kSsspThreads = 256;
+constexpr unsigned kRelaxCtasPerSm = 5;
 // slots per warp range: LG_TUNE_SSSP_RANGE (1024 by default)
 
 __global__ void sssp_init(uint32_t* dist, uint32_t* stamp, uint32_t* fstamp,
@@ -74,7 +75,9 @@ __device__ __forceinline__ void wq_add(bool take, uint32_t item, uint32_t* sbuf,
 // ranges that the grid's warps take in turn, so a hub in the queue is spread
 // over many warps.  ctr[0] near-next length, ctr[1] far length (starts at
 // the current pile size), ctr[2] relaxations.
-__global__ void __launch_bounds__(kSsspThreads)
+// Registers capped for 5 resident CTAs per SM (48, no spills; 62 uncapped):
+// the grid below is exactly the resident CTAs, one wave.
+__global__ void __launch_bounds__(kSsspThreads, kRelaxCtasPerSm)
 sssp_relax(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qlen,
 		uint32_t* dist, uint32_t* stamp, uint32_t* fstamp, uint32_t round, uint32_t epoch,
 		uint32_t hi, uint32_t* near_next, uint32_t* far, unsigned long long* ctr,
@@ -346,7 +349,7 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 	uint32_t* qpos = qcnt + V;
 	int sms = 148;
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
-	const unsigned relax_blocks = (unsigned)sms * 8u;   // persistent over the ranges
+	const unsigned relax_blocks = (unsigned)sms * kRelaxCtasPerSm;   // persistent, one wave
 	const uint32_t range = (uint32_t)tune_value(s->device, LG_TUNE_SSSP_RANGE);
 	const bool dev_out = is_device_pointer(dist);
 	uint32_t* d = dist;
