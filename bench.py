@@ -374,7 +374,7 @@ def run_lg(args):
     if not args.no_autotune:
         t0 = time.time()
         tuning = sn.autotune(["pr_ctas_per_sm", "pr_tile_occ", "ms_heavy", "sssp_split",
-                              "sssp_range"])
+                              "sssp_range", "sssp_levels", "bfs_levels"])
         tuning["seconds"] = time.time() - t0
 
     pr_dev = torch.empty(V, dtype=torch.float64, device=f"cuda:{local}")

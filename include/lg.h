@@ -569,7 +569,14 @@ lg_status lg_adjoint_free(lg_adjoint* tape);
  * on the device and meet at grid barriers; 0 = a launch sequence per level
  * with the direction chosen on the host.  Default 1. */
 #define LG_TUNE_BFS_LEVELS      7
-#define LG_TUNE_COUNT           8
+/* Delta-stepping SSSP: 1 = all rounds, bucket splits and heavy phases in one
+ * cooperative launch whose CTAs apply the host loop's rules on the device
+ * and meet at bounded grid barriers; 0 = a launch sequence per step with the
+ * host reading the counters back.  Default 0: on the R-MAT workloads the one
+ * launch gains 3-8 % with LG_TUNE_SSSP_SPLIT and loses 8 % without (its
+ * relaxation loop holds fewer warps per SM than the per-step kernel). */
+#define LG_TUNE_SSSP_LEVELS     8
+#define LG_TUNE_COUNT           9
 #define LG_TUNE_MAX_DEVICES     64
 lg_status lg_tune_get(int device, int key, int64_t* value);
 lg_status lg_tune_set(int device, int key, int64_t value);

@@ -40,7 +40,8 @@ LG_TUNE_MS_HEAVY = 4
 LG_TUNE_PR_TILE_OCC = 5
 LG_TUNE_SSSP_SPLIT = 6
 LG_TUNE_BFS_LEVELS = 7
-LG_TUNE_COUNT = 8
+LG_TUNE_SSSP_LEVELS = 8
+LG_TUNE_COUNT = 9
 LG_TUNE_MAX_DEVICES = 64
 
 

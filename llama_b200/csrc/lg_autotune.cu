@@ -135,6 +135,11 @@ extern "C" lg_status lg_autotune(lg_snapshot* sn, unsigned keys, lg_tune_trial* 
 			[=, &roots]() {
 				return lg_sssp_delta(sn, roots[0], 32, (uint32_t*)iout, nullptr);
 			}});
+	if ((keys & (1u << LG_TUNE_SSSP_LEVELS)) && weighted)
+		probes.push_back({LG_TUNE_SSSP_LEVELS, {0, 1},
+			[=, &roots]() {
+				return lg_sssp_delta(sn, roots[0], 32, (uint32_t*)iout, nullptr);
+			}});
 	if ((keys & (1u << LG_TUNE_MS_HEAVY)) && sn->flat[1])
 		probes.push_back({LG_TUNE_MS_HEAVY, {128, 256, 512, 1024, 4096},
 			[=, &roots]() {

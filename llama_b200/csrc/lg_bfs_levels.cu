@@ -36,9 +36,10 @@
 //
 // Buffers written inside the kernel (queues, offsets, bitmaps, levels) are
 // read through L2 or by plain loads after a barrier, never through the
-// read-only path.  Every barrier wait is bounded (kWaitNs of the global
+// read-only path.  Every barrier wait is bounded (lg_coop.cuh: kCoopWaitNs of the global
 // timer); a CTA that gives up sets an error flag, leaves, and the host
 // reports LG_ETIMEOUT.
+#include "lg_coop.cuh"
 #include "lg_expand.cuh"
 #include "lg_flat.cuh"
 #include "lg_tune.h"
@@ -56,98 +57,17 @@ constexpr int kLvChunk = 4;            // in-neighbours per vertex per round
 constexpr int kLvSmallPer = 4;         // queue entries per thread of the barrier-free scan
 constexpr uint32_t kLvMaxRange = 1024; // top-down slots per warp range
 constexpr int32_t kLvUnreached = LG_UNREACHED;
-constexpr uint64_t kWaitNs = 1000000000ull;
 constexpr double kAlpha = 14.0, kBeta = 24.0;   // as lg_bfs's host loop
 
 // Control block (device memory; bfs_levels_init resets it).
 struct LvCtl {
 	unsigned long long ctr[3][4];   // per level: [0] frontier size, [1] its out-degree
 	                                // sum, [2] queue fill cursor, [3] unfound rows
-	unsigned int bar_count;
-	unsigned int bar_gen;
-	unsigned int err;               // 1: a barrier wait gave up, 2: slots above 2^32
+	CoopBar bar;                    // err bit 0: a barrier wait gave up, bit 1: slots
+	                                // above 2^32
 	int32_t levels, td, bu, pad;
 	unsigned long long reached, reach_edges;
 };
-
-__device__ __forceinline__ uint64_t global_ns() {
-	uint64_t t;
-	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-	return t;
-}
-
-// Barrier over all CTAs of the cooperative grid (all co-resident).  Thread 0
-// of each CTA publishes the CTA's writes (fence), arrives, and waits for the
-// generation to move on; false once any CTA gave up waiting.
-__device__ bool grid_barrier(LvCtl* c) {
-	__shared__ int s_ok;
-	__syncthreads();
-	if (threadIdx.x == 0) {
-		int ok = 1;
-		volatile unsigned int* gen = &c->bar_gen;
-		const unsigned int g = *gen;
-		__threadfence();
-		if (atomicAdd(&c->bar_count, 1u) == gridDim.x - 1u) {
-			atomicExch(&c->bar_count, 0u);
-			__threadfence();
-			atomicAdd(&c->bar_gen, 1u);
-		} else {
-			const uint64_t t0 = global_ns();
-			while (*gen == g) {
-				if (global_ns() - t0 > kWaitNs) {
-					atomicOr(&c->err, 1u);
-					ok = 0;
-					break;
-				}
-				__nanosleep(64);
-			}
-		}
-		__threadfence();
-		if (*(volatile unsigned int*)&c->err) ok = 0;
-		s_ok = ok;
-	}
-	__syncthreads();
-	return s_ok != 0;
-}
-
-// Sum of x over the CTA, returned to every thread (all threads call it).
-__device__ __forceinline__ unsigned long long block_sum(unsigned long long x) {
-	__shared__ unsigned long long s_part[kLvWarps];
-	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-#pragma unroll
-	for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-	__syncthreads();                     // s_part free from a previous call
-	if (lane == 0) s_part[wid] = x;
-	__syncthreads();
-	unsigned long long t = 0;
-#pragma unroll
-	for (int w = 0; w < kLvWarps; w++) t += s_part[w];
-	return t;
-}
-
-// Exclusive scan of x over the CTA in thread order; *total = the CTA's sum.
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* total) {
-	__shared__ uint32_t s_warp[kLvWarps];
-	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-	uint32_t inc = x;
-#pragma unroll
-	for (int o = 1; o < 32; o <<= 1) {
-		const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-		if (lane >= (uint32_t)o) inc += y;
-	}
-	__syncthreads();
-	if (lane == 31u) s_warp[wid] = inc;
-	__syncthreads();
-	uint32_t before = 0, all = 0;
-#pragma unroll
-	for (int w = 0; w < kLvWarps; w++) {
-		const uint32_t s = s_warp[w];
-		if (w < (int)wid) before += s;
-		all += s;
-	}
-	*total = all;
-	return before + inc - x;
-}
 
 // Appends item[j] for every j with take[j] to out at slots taken from *len:
 // the CTA's count with one atomic, positions in (warp, j, lane) order.
@@ -201,8 +121,8 @@ __global__ void bfs_levels_init(uint32_t root, uint32_t* q0, const uint32_t* out
 			for (int j = 0; j < 4; j++) c->ctr[i][j] = 0;
 		c->ctr[0][0] = 1;
 		c->ctr[0][1] = __ldg(outdeg + root);
-		c->bar_count = 0;
-		c->err = 0;
+		c->bar.count = 0;
+		c->bar.err = 0;
 		c->levels = c->td = c->bu = c->pad = 0;
 		c->reached = c->reach_edges = 0;
 	}
@@ -238,7 +158,7 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 			bits0[w] = w == (root >> 5) ? 1u << (root & 31u) : 0u;
 			bits1[w] = 0u;
 		}
-		if (!grid_barrier(c)) return;
+		if (!grid_barrier(&c->bar)) return;
 	}
 	for (;; cur++) {
 		unsigned long long* now = c->ctr[cur % 3];
@@ -267,7 +187,7 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 					const uint32_t m = w < W ? bits[w] : 0u;
 					const uint32_t nb = __popc(m);
 					uint32_t all;
-					const uint32_t ex = block_exclusive_scan(nb, &all);
+					const uint32_t ex = block_exclusive_scan<kLvWarps>(nb, &all);
 					__shared__ unsigned long long s_qbase;
 					if (tid == 0) s_qbase = all ? atomicAdd(now + 2, (unsigned long long)all) : 0ull;
 					__syncthreads();
@@ -279,7 +199,7 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 						q[pos++] = w * 32u + (uint32_t)b;
 					}
 				}
-				if (!grid_barrier(c)) return;
+				if (!grid_barrier(&c->bar)) return;
 				have_queue = true;
 			}
 			const uint32_t n = (uint32_t)qlen;
@@ -297,12 +217,12 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 					kc[j] = i < n ? vertex_slots(out, __ldcg(q + i), &f0) : 0u;
 					sum += kc[j];
 				}
-				if (block_sum(sum) >= (1ull << 32)) {
-					if (tid == 0) atomicOr(&c->err, 2u);
+				if (block_sum<kLvWarps>(sum) >= (1ull << 32)) {
+					if (tid == 0) atomicOr(&c->bar.err, 2u);
 					return;                      // every CTA sees the same total
 				}
 				uint32_t all;
-				uint32_t ex = block_exclusive_scan((uint32_t)sum, &all);
+				uint32_t ex = block_exclusive_scan<kLvWarps>((uint32_t)sum, &all);
 #pragma unroll
 				for (int j = 0; j < kLvSmallPer; j++) {
 					const uint32_t i = tid * kLvSmallPer + j;
@@ -323,9 +243,9 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 					fcnt[i] = k;
 					s += k;
 				}
-				s = block_sum(s);
+				s = block_sum<kLvWarps>(s);
 				if (tid == 0) bsum[blockIdx.x] = s;
-				if (!grid_barrier(c)) return;
+				if (!grid_barrier(&c->bar)) return;
 				// phase B: offsets (every CTA forms the same total)
 				unsigned long long pre = 0;
 				for (uint32_t b = tid; b < gridDim.x; b += blockDim.x) {
@@ -333,10 +253,10 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 					tot += x;
 					if (b < blockIdx.x) pre += x;
 				}
-				pre = block_sum(pre);
-				tot = block_sum(tot);
+				pre = block_sum<kLvWarps>(pre);
+				tot = block_sum<kLvWarps>(tot);
 				if (tot >= (1ull << 32)) {
-					if (tid == 0) atomicOr(&c->err, 2u);
+					if (tid == 0) atomicOr(&c->bar.err, 2u);
 					return;                      // every CTA sees the same total
 				}
 				uint32_t run = (uint32_t)pre;
@@ -344,12 +264,12 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 					const uint32_t i = p + tid;
 					const uint32_t x = i < c1 ? __ldcg(fcnt + i) : 0u;
 					uint32_t piece;
-					const uint32_t ex = block_exclusive_scan(x, &piece);
+					const uint32_t ex = block_exclusive_scan<kLvWarps>(x, &piece);
 					if (i < c1) fpos[i] = run + ex;
 					run += piece;
 				}
 				if (blockIdx.x == gridDim.x - 1u && tid == 0) fpos[n] = (uint32_t)tot;
-				if (!grid_barrier(c)) return;
+				if (!grid_barrier(&c->bar)) return;
 			}
 			// phase C: expand the queue over balanced slot ranges
 			const uint32_t total = (uint32_t)tot;
@@ -381,7 +301,7 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 				for (uint32_t r = gwarp; r < nranges; r += nwarps)
 					range_for_each<1>(out, q, fpos, n, total, nranges, range, r, visit);
 			}
-			mfn = block_sum(mfn);
+			mfn = block_sum<kLvWarps>(mfn);
 			if (tid == 0 && mfn) atomicAdd(nxt + 1, mfn);
 			td++;
 		} else {
@@ -470,15 +390,15 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 				for (int j = 0; j < kLvVerts; j++) stay[j] = keep[j] && !found[j];
 				block_append_rows(stay, row, lout, nxt + 3);
 			}
-			cnt = block_sum(cnt);
-			mfn = block_sum(mfn);
+			cnt = block_sum<kLvWarps>(cnt);
+			mfn = block_sum<kLvWarps>(mfn);
 			if (tid == 0) {
 				if (cnt) atomicAdd(nxt + 0, cnt);
 				if (mfn) atomicAdd(nxt + 1, mfn);
 			}
 			bu++;
 		}
-		if (!grid_barrier(c)) return;
+		if (!grid_barrier(&c->bar)) return;
 		if (top_down) {
 			uint32_t* t = q; q = nq; nq = t;
 			have_queue = true;
@@ -498,28 +418,15 @@ bfs_levels(SnapCsr out, const uint32_t* nz_rows, const uint32_t* nz_off, uint32_
 	}
 }
 
-struct CoopInfo {
-	bool probed = false;
-	int grid = 0;            // co-resident CTAs of bfs_levels, 0 = no cooperative launch
-};
 std::mutex g_coop_mu;
-CoopInfo g_coop[LG_TUNE_MAX_DEVICES];
+int g_coop[LG_TUNE_MAX_DEVICES];          // co-resident CTAs of bfs_levels + 1, 0 = not probed
 
 int coop_grid(int device) {
 	std::lock_guard<std::mutex> lk(g_coop_mu);
 	if (device < 0 || device >= LG_TUNE_MAX_DEVICES) return 0;
-	CoopInfo& ci = g_coop[device];
-	if (!ci.probed) {
-		ci.probed = true;
-		int coop = 0, sms = 0, per_sm = 0;
-		if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) == cudaSuccess &&
-				cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
-				cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_levels, kLvThreads, 0) ==
-						cudaSuccess && coop && sms > 0 && per_sm > 0)
-			ci.grid = sms * per_sm;
-		cudaGetLastError();
-	}
-	return ci.grid;
+	if (!g_coop[device])
+		g_coop[device] = 1 + coop_grid_size((const void*)bfs_levels, kLvThreads, device);
+	return g_coop[device] - 1;
 }
 
 } // namespace
@@ -580,10 +487,10 @@ lg_status bfs_levels_run(lg_snapshot* sn, uint32_t root, int32_t* lvl, lg_bfs_re
 	LG_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(h), cudaMemcpyDeviceToHost, st), "d2h");
 	LG_CUDA(cudaStreamSynchronize(st), "bfs_levels");
 	s->d2h_bytes += sizeof(h);
-	if (h.err & 1u)
+	if (h.bar.err & 1u)
 		return set_error(LG_ETIMEOUT, "bfs: a grid barrier wait ran out (%d levels done)",
 				h.levels);
-	if (h.err & 2u)
+	if (h.bar.err & 2u)
 		return set_error(LG_ENOTSUP, "bfs: a frontier holds 2^32 or more slots");
 	if (result) {
 		result->reached = h.reached;

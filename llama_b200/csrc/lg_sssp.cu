@@ -17,6 +17,8 @@
 // and weights in one array each, no deletion bits) instead of the levels.
 #include "lg_expand.cuh"
 #include "lg_flat.cuh"
+#include "lg_sssp.cuh"
+#include "lg_sssp_levels.h"
 #include "lg_tune.h"
 
 #include <cstring>
@@ -24,7 +26,6 @@
 
 namespace lg {
 
-constexpr uint32_t kInf = LG_UNREACHED;
 constexpr int kSsspThreads = 256;
 constexpr unsigned kRelaxCtasPerSm = 5;
 // slots per warp range: LG_TUNE_SSSP_RANGE (1024 by default)
@@ -38,35 +39,6 @@ __global__ void sssp_init(uint32_t* dist, uint32_t* stamp, uint32_t* fstamp,
 		fstamp[v] = 0xffffffffu;
 	}
 	if (v == 0) queue[0] = root;
-}
-
-// Per-warp staging of queue appends in shared memory: items collect in a
-// kPushBuf-entry buffer and go to the global queue kPushBuf at a time with
-// one atomic, instead of one atomic on the same counter per 32 items (which
-// serialises in L2 when most warps append).  n is warp-uniform.
-constexpr uint32_t kPushBuf = 128;
-
-__device__ __forceinline__ void wq_flush(uint32_t* sbuf, uint32_t& n, uint32_t* queue,
-		unsigned long long* len) {
-	if (n == 0) return;
-	const uint32_t lane = threadIdx.x & 31u;
-	__syncwarp();
-	unsigned long long base = 0;
-	if (lane == 0) base = atomicAdd(len, (unsigned long long)n);
-	base = __shfl_sync(0xffffffffu, base, 0);
-	for (uint32_t i = lane; i < n; i += 32u) queue[base + i] = sbuf[i];
-	__syncwarp();
-	n = 0;
-}
-
-__device__ __forceinline__ void wq_add(bool take, uint32_t item, uint32_t* sbuf, uint32_t& n,
-		uint32_t* queue, unsigned long long* len) {
-	const unsigned m = __ballot_sync(0xffffffffu, take);
-	if (!m) return;
-	if (n + (uint32_t)__popc(m) > kPushBuf) wq_flush(sbuf, n, queue, len);
-	const uint32_t lane = threadIdx.x & 31u;
-	if (take) sbuf[n + __popc(m & ((1u << lane) - 1u))] = item;
-	n += __popc(m);
 }
 
 // One relaxation round over the near queue.  The queue's slot space
@@ -84,39 +56,11 @@ sssp_relax(SnapCsr out, const uint32_t* queue, const uint32_t* pos, uint32_t qle
 		uint32_t range_max) {
 	__shared__ uint32_t sbuf[kSsspThreads / 32][2][kPushBuf];
 	const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-	const uint32_t total = __ldg(pos + qlen);
 	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-	// ranges of at most `range_max` slots, fewer when the queue's slots would
-	// not give every warp one: late rounds queue 10^5 - 10^6 vertices with
-	// a slot or less each, and fixed-size ranges left most warps idle while a
-	// few walked thousands of entries
-	uint32_t range = (uint32_t)(((uint64_t)total + nwarps - 1) / nwarps);
-	range = min(max((range + 31u) & ~31u, 32u), range_max);
-	const uint32_t nranges = (total + range - 1) / range;
-	unsigned long long relax = 0;
-	uint32_t nn = 0, nf = 0;       // staged near / far appends of this warp
-	for (uint32_t r = warp; r < nranges; r += nwarps) {
-		range_for_each(out, queue, pos, qlen, total, nranges, range, r,
-			[&](bool act, uint32_t, uint32_t ov, uint32_t nbr, uint32_t lv, uint32_t idx) {
-				bool to_near = false, to_far = false;
-				if (act) {
-					const uint32_t nd = __ldcg(dist + ov) + __ldg(out.lt->w[lv] + idx);
-					if (nd < __ldcg(dist + nbr)) {
-						const uint32_t old = atomicMin(dist + nbr, nd);
-						relax++;
-						if (nd < old) {
-							if (nd < hi) to_near = atomicExch(stamp + nbr, round) != round;
-							else to_far = atomicExch(fstamp + nbr, epoch) != epoch;
-						}
-					}
-				}
-				wq_add(to_near, nbr, sbuf[wid][0], nn, near_next, ctr);
-				wq_add(to_far, nbr, sbuf[wid][1], nf, far, ctr + 1);
-			});
-	}
-	wq_flush(sbuf[wid][0], nn, near_next, ctr);
-	wq_flush(sbuf[wid][1], nf, far, ctr + 1);
+	unsigned long long relax = sssp_relax_ranges<0>(out, queue, pos, qlen, __ldg(pos + qlen),
+			range_max, warp, nwarps, dist, stamp, fstamp, round, epoch, hi, near_next, ctr, far,
+			ctr + 1, sbuf[wid][0], sbuf[wid][1]);
 	for (int o = 16; o > 0; o >>= 1) relax += __shfl_down_sync(0xffffffffu, relax, o);
 	if (lane == 0 && relax) atomicAdd(ctr + 2, relax);
 }
@@ -132,24 +76,9 @@ sssp_split_far(const uint32_t* far, unsigned long long n,
 		unsigned long long* ctr) {
 	__shared__ uint32_t sbuf[kSsspThreads / 32][2][kPushBuf];
 	const uint32_t wid = threadIdx.x >> 5;
-	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-	uint32_t nn = 0, nk = 0;
-	unsigned long long m = ~0ull;
-	// whole warps loop together (the bound is rounded up to the stride)
-	const uint64_t end = (n + 31) & ~31ull;
-	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
-		uint32_t v = 0, d = kInf;
-		if (i < n) { v = far[i]; d = __ldcg(dist + v); }
-		const bool near_take = i < n && d >= lo && d < hi
-			&& atomicExch(stamp + v, round) != round;
-		const bool keep_take = i < n && d >= hi && d < kInf
-			&& atomicExch(fstamp + v, epoch) != epoch;
-		wq_add(near_take, v, sbuf[wid][0], nn, near, ctr);
-		wq_add(keep_take, v, sbuf[wid][1], nk, keep, ctr + 1);
-		if (keep_take) m = min(m, (unsigned long long)d);
-	}
-	wq_flush(sbuf[wid][0], nn, near, ctr);
-	wq_flush(sbuf[wid][1], nk, keep, ctr + 1);
+	unsigned long long m = sssp_split_far_body<0>(far, n, dist, stamp, fstamp, round, epoch,
+			lo, hi, near, ctr, keep, ctr + 1, sbuf[wid][0], sbuf[wid][1],
+			(uint64_t)blockIdx.x * blockDim.x + threadIdx.x, (uint64_t)gridDim.x * blockDim.x);
 	for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_down_sync(0xffffffffu, m, o));
 	if ((threadIdx.x & 31) == 0 && m != ~0ull) atomicMin(ctr + 2, m);
 }
@@ -209,16 +138,8 @@ __global__ void sssp_iota(uint32_t* a, uint64_t n) {
 __global__ void sssp_collect(const uint32_t* q, uint32_t n, uint32_t* bstamp, uint32_t bucket,
 		uint32_t* blist, unsigned long long* ctr) {
 	__shared__ uint32_t sbuf[kSsspThreads / 32][kPushBuf];
-	const uint32_t wid = threadIdx.x >> 5;
-	uint32_t nn = 0;
-	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-	const uint64_t end = ((uint64_t)n + 31) & ~31ull;
-	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
-		const uint32_t v = i < n ? q[i] : 0u;
-		const bool take = i < n && atomicExch(bstamp + v, bucket) != bucket;
-		wq_add(take, v, sbuf[wid], nn, blist, ctr + 3);
-	}
-	wq_flush(sbuf[wid], nn, blist, ctr + 3);
+	sssp_collect_body<0>(q, n, bstamp, bucket, blist, ctr + 3, sbuf[threadIdx.x >> 5],
+			(uint64_t)blockIdx.x * blockDim.x + threadIdx.x, (uint64_t)gridDim.x * blockDim.x);
 }
 
 __global__ void sssp_reach(const uint32_t* dist, const uint32_t* outdeg, uint64_t V,
@@ -395,6 +316,30 @@ extern "C" lg_status lg_sssp_delta(lg_snapshot* sn, int64_t root, uint32_t delta
 	unsigned long long* h = hw;              // 4 words read back
 	unsigned long long* init = hw + 4;       // 4 words written
 	LG_CUDA(cudaMemsetAsync(ctr, 0, 4 * sizeof(unsigned long long), st), "memset");
+	// the same rounds in one cooperative launch (LG_TUNE_SSSP_LEVELS)
+	bool one_launch = false;
+	if (tune_value(s->device, LG_TUNE_SSSP_LEVELS)) {
+		SsspLevelsArgs a;
+		a.out = out;
+		a.heavy = heavy;
+		a.split = split ? 1 : 0;
+		a.q = q; a.qn = qn; a.far = far; a.far2 = far2;
+		a.dist = d; a.stamp = stamp; a.fstamp = fstamp; a.bstamp = bstamp; a.blist = blist;
+		a.cnt = qcnt; a.pos = qpos;
+		a.bsum = nullptr;
+		a.V = V;
+		a.delta = delta;
+		a.range_max = range;
+		int r = 0, b = 0;
+		uint64_t rx = 0;
+		LG_TRY(sssp_levels_run(s, a, sc[11], &r, &b, &rx, &one_launch));
+		if (one_launch) {
+			round = (uint32_t)r;
+			buckets = b;
+			relaxations = rx;
+			qlen = flen = blen = 0;
+		}
+	}
 	while (qlen > 0 || flen > 0 || blen > 0) {
 		if (qlen == 0 && blen > 0) {
 			// the bucket has drained: its settled vertices relax their

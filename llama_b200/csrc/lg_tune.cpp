@@ -25,6 +25,7 @@ const Limits kLimits[LG_TUNE_COUNT] = {
 	{0, 8, 0},          // LG_TUNE_PR_TILE_OCC (0 or 8)
 	{0, 1, 0},          // LG_TUNE_SSSP_SPLIT
 	{0, 1, 1},          // LG_TUNE_BFS_LEVELS
+	{0, 1, 0},          // LG_TUNE_SSSP_LEVELS
 };
 
 std::mutex g_mu;

@@ -272,7 +272,8 @@ TUNABLES = {"pr_ctas_per_sm": _lib.LG_TUNE_PR_CTAS_PER_SM,
             "ms_heavy": _lib.LG_TUNE_MS_HEAVY,
             "pr_tile_occ": _lib.LG_TUNE_PR_TILE_OCC,
             "sssp_split": _lib.LG_TUNE_SSSP_SPLIT,
-            "bfs_levels": _lib.LG_TUNE_BFS_LEVELS}
+            "bfs_levels": _lib.LG_TUNE_BFS_LEVELS,
+            "sssp_levels": _lib.LG_TUNE_SSSP_LEVELS}
 
 
 def tune_set(device, name, value):

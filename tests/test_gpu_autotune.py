@@ -77,7 +77,7 @@ def test_autotune_keeps_the_fastest_measured_value(store):
         # the flat in-CSR made for the probes is released again
         assert not sn.is_flat(1)
     assert set(res) == {"pr_ctas_per_sm", "ppr_ktile", "ppr_range", "sssp_range", "ms_heavy",
-                        "pr_tile_occ", "sssp_split", "bfs_levels"}
+                        "pr_tile_occ", "sssp_split", "bfs_levels", "sssp_levels"}
     for name, r in res.items():
         assert r["chosen"] in r["ms"]
         assert all(ms > 0 for ms in r["ms"].values())

@@ -6,7 +6,8 @@ from llama_b200 import LgError
 from llama_b200.graph import TUNABLES, tune_get, tune_reset, tune_set
 
 DEFAULTS = {"pr_ctas_per_sm": 0, "ppr_ktile": 256, "ppr_range": 2048, "sssp_range": 1024,
-            "ms_heavy": 512, "pr_tile_occ": 0, "sssp_split": 0, "bfs_levels": 1}
+            "ms_heavy": 512, "pr_tile_occ": 0, "sssp_split": 0, "bfs_levels": 1,
+            "sssp_levels": 0}
 
 
 def test_defaults_set_and_reset():
