@@ -18,6 +18,7 @@
 // vertex, and labels do not depend on thread order.
 #include "lg_device.cuh"
 #include "lg_expand.cuh"
+#include "lg_queue.cuh"
 
 namespace lg {
 
@@ -25,17 +26,7 @@ constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kSccRange = 1024;
 constexpr int kSccThreads = 256;
 
-__device__ __forceinline__ void scc_push(bool take, uint32_t item, uint32_t* list,
-		unsigned long long* len) {
-	const unsigned m = __ballot_sync(0xffffffffu, take);
-	if (!m) return;
-	const uint32_t lane = threadIdx.x & 31u;
-	const int leader = __ffs(m) - 1;
-	unsigned long long base = 0;
-	if ((int)lane == leader) base = atomicAdd(len, (unsigned long long)__popc(m));
-	base = __shfl_sync(0xffffffffu, base, leader);
-	if (take) list[base + __popc(m & ((1u << lane) - 1u))] = item;
-}
+constexpr int kSccListThreads = 256;   // CTA size of the per-vertex list kernels
 
 // Trim: vertices without live in- or out-edges are singletons; the others
 // form the initial remaining list.  ctr[0] = remaining count.
@@ -50,7 +41,7 @@ __global__ void scc_trim(const uint32_t* outdeg, const uint32_t* indeg, uint64_t
 		mark[v] = 0;
 		stamp[v] = 0;
 	}
-	scc_push(keep, (uint32_t)v, rem, ctr);
+	block_push<kSccListThreads>(keep, (uint32_t)v, rem, ctr);
 }
 
 __global__ void scc_color_init(const uint32_t* rem, uint32_t n, uint32_t* color) {
@@ -63,8 +54,11 @@ __global__ void __launch_bounds__(kSccThreads)
 scc_propagate(SnapCsr out, const uint32_t* wl, const uint32_t* pos, uint32_t n,
 		uint32_t total, uint32_t nranges, const uint32_t* label, uint32_t* color,
 		uint32_t* stamp, uint32_t round, uint32_t* next, unsigned long long* ctr) {
+	__shared__ uint32_t sbuf[kSccThreads / 32][kPushBuf];
 	const uint64_t r = (uint64_t)blockIdx.x * (kSccThreads / 32) + (threadIdx.x >> 5);
 	if (r >= nranges) return;
+	uint32_t* sb = sbuf[threadIdx.x >> 5];
+	uint32_t nb = 0;
 	range_for_each(out, wl, pos, n, total, nranges, kSccRange, (uint32_t)r,
 		[&](bool act, uint32_t own, uint32_t v, uint32_t w, uint32_t, uint32_t) {
 			bool push = false;
@@ -75,8 +69,9 @@ scc_propagate(SnapCsr out, const uint32_t* wl, const uint32_t* pos, uint32_t n,
 					if (c < old) push = atomicExch(stamp + w, round) != round;
 				}
 			}
-			scc_push(push, w, next, ctr);
+			wq_add(push, w, sb, nb, next, ctr);
 		});
+	wq_flush(sb, nb, next, ctr);
 }
 
 // Roots: remaining vertices whose colour is their own id start the backward
@@ -91,7 +86,7 @@ __global__ void scc_roots(const uint32_t* rem, uint32_t n, const uint32_t* color
 		root = color[v] == v;
 		if (root) mark[v] = round;
 	}
-	scc_push(root, v, frontier, ctr);
+	block_push<kSccListThreads>(root, v, frontier, ctr);
 }
 
 // Backward traversal over in-edges within a colour.
@@ -99,16 +94,20 @@ __global__ void __launch_bounds__(kSccThreads)
 scc_backward(SnapCsr in, const uint32_t* fr, const uint32_t* pos, uint32_t n,
 		uint32_t total, uint32_t nranges, const uint32_t* label, const uint32_t* color,
 		uint32_t* mark, uint32_t round, uint32_t* next, unsigned long long* ctr) {
+	__shared__ uint32_t sbuf[kSccThreads / 32][kPushBuf];
 	const uint64_t r = (uint64_t)blockIdx.x * (kSccThreads / 32) + (threadIdx.x >> 5);
 	if (r >= nranges) return;
+	uint32_t* sb = sbuf[threadIdx.x >> 5];
+	uint32_t nb = 0;
 	range_for_each(in, fr, pos, n, total, nranges, kSccRange, (uint32_t)r,
 		[&](bool act, uint32_t own, uint32_t v, uint32_t u, uint32_t, uint32_t) {
 			bool push = false;
 			if (act && __ldcg(label + u) == kNone && __ldcg(mark + u) != round
 					&& __ldcg(color + u) == __ldcg(color + v))
 				push = atomicExch(mark + u, round) != round;
-			scc_push(push, u, next, ctr);
+			wq_add(push, u, sb, nb, next, ctr);
 		});
+	wq_flush(sb, nb, next, ctr);
 }
 
 // Collected vertices get their label; the rest stay for the next round.
@@ -123,7 +122,7 @@ __global__ void scc_collect(const uint32_t* rem, uint32_t n, const uint32_t* col
 		if (mark[v] == round) label[v] = color[v];
 		else keep = true;
 	}
-	scc_push(keep, v, rem_next, ctr);
+	block_push<kSccListThreads>(keep, v, rem_next, ctr);
 }
 
 __global__ void scc_output(const uint32_t* label, uint64_t V, long long* out,
@@ -195,7 +194,7 @@ extern "C" lg_status lg_scc(lg_snapshot* sn, int64_t* labels, lg_scc_result* res
 	uint32_t* stp = stamp.as<uint32_t>();
 
 	LG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), st), "memset");
-	scc_trim<<<grid_for(V, 256), 256, 0, st>>>(sn->out.deg.as<uint32_t>(),
+	scc_trim<<<grid_for(V, kSccListThreads), kSccListThreads, 0, st>>>(sn->out.deg.as<uint32_t>(),
 			sn->in.deg.as<uint32_t>(), V, lab, mk, stp, rem.as<uint32_t>(), ctr);
 	LG_CUDA(cudaGetLastError(), "scc_trim");
 	s->launches++;
@@ -229,7 +228,7 @@ extern "C" lg_status lg_scc(lg_snapshot* sn, int64_t* labels, lg_scc_result* res
 		}
 		// backward traversal from the roots
 		LG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), st), "memset");
-		scc_roots<<<grid_for(n_rem, 256), 256, 0, st>>>(R, (uint32_t)n_rem, col, mk, round,
+		scc_roots<<<grid_for(n_rem, kSccListThreads), kSccListThreads, 0, st>>>(R, (uint32_t)n_rem, col, mk, round,
 				W, ctr);
 		LG_CUDA(cudaGetLastError(), "scc_roots");
 		s->launches++;
@@ -247,7 +246,7 @@ extern "C" lg_status lg_scc(lg_snapshot* sn, int64_t* labels, lg_scc_result* res
 			steps++;
 		}
 		LG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long), st), "memset");
-		scc_collect<<<grid_for(n_rem, 256), 256, 0, st>>>(R, (uint32_t)n_rem, col, mk, round,
+		scc_collect<<<grid_for(n_rem, kSccListThreads), kSccListThreads, 0, st>>>(R, (uint32_t)n_rem, col, mk, round,
 				lab, R2, ctr);
 		LG_CUDA(cudaGetLastError(), "scc_collect");
 		s->launches++;

@@ -6,39 +6,11 @@
 #define LG_SSSP_CUH_
 
 #include "lg_expand.cuh"
+#include "lg_queue.cuh"
 
 namespace lg {
 
 constexpr uint32_t kInf = LG_UNREACHED;
-
-// Per-warp staging of queue appends in shared memory: items collect in a
-// kPushBuf-entry buffer and go to the global queue kPushBuf at a time with
-// one atomic, instead of one atomic on the same counter per 32 items (which
-// serialises in L2 when most warps append).  n is warp-uniform.
-constexpr uint32_t kPushBuf = 128;
-
-__device__ __forceinline__ void wq_flush(uint32_t* sbuf, uint32_t& n, uint32_t* queue,
-		unsigned long long* len) {
-	if (n == 0) return;
-	const uint32_t lane = threadIdx.x & 31u;
-	__syncwarp();
-	unsigned long long base = 0;
-	if (lane == 0) base = atomicAdd(len, (unsigned long long)n);
-	base = __shfl_sync(0xffffffffu, base, 0);
-	for (uint32_t i = lane; i < n; i += 32u) queue[base + i] = sbuf[i];
-	__syncwarp();
-	n = 0;
-}
-
-__device__ __forceinline__ void wq_add(bool take, uint32_t item, uint32_t* sbuf, uint32_t& n,
-		uint32_t* queue, unsigned long long* len) {
-	const unsigned m = __ballot_sync(0xffffffffu, take);
-	if (!m) return;
-	if (n + (uint32_t)__popc(m) > kPushBuf) wq_flush(sbuf, n, queue, len);
-	const uint32_t lane = threadIdx.x & 31u;
-	if (take) sbuf[n + __popc(m & ((1u << lane) - 1u))] = item;
-	n += __popc(m);
-}
 
 // Loads of the near queue / far pile entries: plain (kLd != 1) or through
 // L2 (kLd == 1, for buffers rewritten earlier in the same launch).
