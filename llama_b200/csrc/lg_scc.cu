@@ -133,8 +133,14 @@ __global__ void scc_output(const uint32_t* label, uint64_t V, long long* out,
 		out[v] = (long long)label[v];
 		head = label[v] == (uint32_t)v;
 	}
+	// one counter atomic per CTA (kSccListThreads threads)
+	__shared__ unsigned int s_heads;
+	if (threadIdx.x == 0) s_heads = 0;
+	__syncthreads();
 	const unsigned m = __ballot_sync(0xffffffffu, head);
-	if ((threadIdx.x & 31) == 0 && m) atomicAdd(comps, (unsigned long long)__popc(m));
+	if ((threadIdx.x & 31) == 0 && m) atomicAdd(&s_heads, (unsigned int)__popc(m));
+	__syncthreads();
+	if (threadIdx.x == 0 && s_heads) atomicAdd(comps, (unsigned long long)s_heads);
 }
 
 } // namespace lg
@@ -260,7 +266,7 @@ extern "C" lg_status lg_scc(lg_snapshot* sn, int64_t* labels, lg_scc_result* res
 	long long* o = (long long*)labels;
 	if (!dev_out) { LG_TRY(outb.reserve(V * 8)); o = outb.as<long long>(); }
 	LG_CUDA(cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned long long), st), "memset");
-	scc_output<<<grid_for(V, 256), 256, 0, st>>>(lab, V, o, ctr + 1);
+	scc_output<<<grid_for(V, kSccListThreads), kSccListThreads, 0, st>>>(lab, V, o, ctr + 1);
 	LG_CUDA(cudaGetLastError(), "scc_output");
 	s->launches++;
 	uint64_t comps = 0;

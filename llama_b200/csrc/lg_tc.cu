@@ -37,11 +37,17 @@ __global__ void tc_rank(const uint32_t* out_deg, const uint32_t* in_deg, uint64_
 }
 
 // Every live arc of the out-CSR, over balanced 1024-slot ranges of all
-// vertices' slots (pos = the snapshot's slot prefix), becomes an oriented key.
+// vertices' slots (pos = the snapshot's slot prefix), becomes an oriented key;
+// each warp stages its keys in shared memory and appends kTcStage at a time
+// (one counter atomic per batch, not per 32 slots).
 constexpr uint32_t kTcRange = 1024;
+constexpr uint32_t kTcStage = 256;
 __global__ void __launch_bounds__(kTcThreads)
 tc_emit(SnapCsr out, const uint32_t* pos, uint32_t total, const uint32_t* rk,
 		unsigned long long* keys, unsigned long long* n_keys) {
+	__shared__ unsigned long long stage[kTcThreads / 32][kTcStage];
+	unsigned long long* sb = stage[threadIdx.x >> 5];
+	uint32_t ns = 0;                       // staged keys of this warp (warp-uniform)
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint32_t nranges = (total + kTcRange - 1) / kTcRange;
 	const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -56,15 +62,28 @@ tc_emit(SnapCsr out, const uint32_t* pos, uint32_t total, const uint32_t* rk,
 				if (rank_less(b, a, rk)) { a = nbr; b = src; }
 				key = ((unsigned long long)a << 32) | b;
 			}
-			unsigned m = __ballot_sync(0xffffffffu, take);
+			const unsigned m = __ballot_sync(0xffffffffu, take);
 			if (m) {
-				const int leader = __ffs(m) - 1;
-				unsigned long long base = 0;
-				if ((int)lane == leader) base = atomicAdd(n_keys, (unsigned long long)__popc(m));
-				base = __shfl_sync(0xffffffffu, base, leader);
-				if (take) keys[base + __popc(m & ((1u << lane) - 1u))] = key;
+				if (ns + (uint32_t)__popc(m) > kTcStage) {
+					__syncwarp();
+					unsigned long long base = 0;
+					if (lane == 0) base = atomicAdd(n_keys, (unsigned long long)ns);
+					base = __shfl_sync(0xffffffffu, base, 0);
+					for (uint32_t i = lane; i < ns; i += 32) keys[base + i] = sb[i];
+					__syncwarp();
+					ns = 0;
+				}
+				if (take) sb[ns + __popc(m & ((1u << lane) - 1u))] = key;
+				ns += __popc(m);
 			}
 		});
+	if (ns) {
+		__syncwarp();
+		unsigned long long base = 0;
+		if (lane == 0) base = atomicAdd(n_keys, (unsigned long long)ns);
+		base = __shfl_sync(0xffffffffu, base, 0);
+		for (uint32_t i = lane; i < ns; i += 32) keys[base + i] = sb[i];
+	}
 }
 
 // off[v] = first oriented edge whose source is >= v
