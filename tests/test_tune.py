@@ -25,7 +25,9 @@ def test_defaults_set_and_reset():
 
 @pytest.mark.parametrize("name,value", [("pr_ctas_per_sm", -1), ("pr_ctas_per_sm", 33),
                                         ("ppr_ktile", 16), ("ppr_range", 100),
-                                        ("sssp_range", 1 << 20), ("ms_heavy", 8)])
+                                        ("sssp_range", 1 << 20), ("ms_heavy", 8),
+                                        ("pr_tile_occ", 9), ("sssp_split", 2),
+                                        ("bfs_levels", 2), ("sssp_levels", -1)])
 def test_out_of_range_values_are_rejected(name, value):
     with pytest.raises(LgError):
         tune_set(0, name, value)
